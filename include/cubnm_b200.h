@@ -1,0 +1,170 @@
+/*
+ * cubnm_b200 C ABI -- the drop-in boundary of the B200 simulation path.
+ *
+ * The reference exposes this path as the CPython extension `cubnm.core`
+ * (src/ext/core.cpp:507-626) with three functions: run_simulations, init and
+ * set_const.  This header restates that boundary as plain C: pointers and
+ * sizes, status codes instead of exceptions, no Python or torch types.  A thin
+ * binding (ctypes, cgo, JNI, ...) rebuilds the `cubnm.core` module on top of it.
+ *
+ * Array layouts follow the reference exactly (row-major, C order):
+ *   sc               [n_scs][nodes*nodes]    rows = source node, cols = target
+ *   sc_indices       [n_sims]                int32, index into sc
+ *   sc_dist          [nodes*nodes]           tract lengths (mm), used with do_delay
+ *   global_params    [n_global][n_sims]      e.g. rWW: G
+ *   regional_params  [n_regional][n_sims*nodes]  sim-major, node-minor
+ *   v_list           [n_sims]                conduction velocity (m/s = mm/ms)
+ * Outputs (caller-allocated, sized by cbnm_query_sizes):
+ *   sim_bold         [n_sims][bold_len*nodes]   volume-major per simulation
+ *   sim_fc_trils     [n_sims][n_pairs]          lower triangle, np.tril_indices(n,-1) order
+ *   sim_fcd_trils    [n_sims][n_window_pairs]   lower triangle of the window-by-window matrix
+ *   sim_states       [n_state_vars][n_sims][nodes (*states_len if states_ts)]
+ *   global_bools     [n_global_out_bool][n_sims]  (uint8, 0/1)
+ *   global_ints      [n_global_out_int][n_sims]
+ *   noise            [noise_size]; shuffled_nodes [noise_repeats][nodes];
+ *   shuffled_ts      [noise_repeats][noise_bw_it]
+ *
+ * Thread safety: like the reference (a process-global model object,
+ * core.cpp:57-58), the library keeps one session per process; calls must not
+ * overlap.  Errors return a non-zero status; cbnm_last_error() describes it.
+ */
+#ifndef CUBNM_B200_H
+#define CUBNM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CBNM_OK 0
+#define CBNM_ERR_ARG 1          /* invalid argument or size */
+#define CBNM_ERR_MODEL 2        /* unknown model name */
+#define CBNM_ERR_CONFIG 3       /* configuration rejected (e.g. no FC windows) */
+#define CBNM_ERR_CUDA 4         /* CUDA runtime error; message starts with "CUDA Error" */
+#define CBNM_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
+#define CBNM_ERR_UNSUPPORTED 6  /* request outside what this build implements */
+
+/* Arguments of one run; positional arguments of core.cpp:202-225 in order. */
+typedef struct cbnm_run_args {
+    const char *model_name;            /* "rWW", "WC", "JR", "Kuramoto", "rWWEx" */
+    const double *sc;                  /* [n_scs][nodes*nodes] */
+    int n_scs;
+    const int32_t *sc_indices;         /* [n_sims] */
+    const double *sc_dist;             /* [nodes*nodes] */
+    double *global_params;             /* [n_global][n_sims]; written back when the model modifies params */
+    double *regional_params;           /* [n_regional][n_sims*nodes]; idem (rWW FIC writes wIE) */
+    const double *v_list;              /* [n_sims] */
+    const char *const *config_keys;    /* model_config dict as parallel key/value string arrays */
+    const char *const *config_values;
+    int n_config;
+    int ext_out;                       /* always 1 in the reference's caller (base.py:736) */
+    int states_ts;
+    int noise_out;
+    int do_delay;
+    int force_reinit;
+    int use_cpu;                       /* must be 0: this library has no CPU path */
+    int n_sims;
+    int nodes;
+    int time_steps;                    /* duration in ms */
+    int bold_tr;                       /* ms */
+    int states_sampling;               /* ms */
+    int sim_seed;
+    double dt;                         /* model step, ms */
+    double bw_dt;                      /* Balloon-Windkessel step, ms */
+} cbnm_run_args;
+
+/* Output sizes for a given set of arguments (core.cpp:336-349). */
+typedef struct cbnm_sizes {
+    int n_global_params;
+    int n_regional_params;
+    int n_state_vars;
+    int n_global_out_bool;
+    int n_global_out_int;
+    int bold_len;
+    int n_pairs;
+    int n_windows;
+    int n_window_pairs;
+    int states_len;
+    int do_fc;
+    int do_fcd;
+    int modifies_params;
+    int noise_repeats;
+    int noise_bw_it;
+    int64_t noise_size;
+} cbnm_sizes;
+
+typedef struct cbnm_outputs {
+    double *sim_bold;
+    double *sim_fc_trils;      /* may be NULL when do_fc is off */
+    double *sim_fcd_trils;     /* may be NULL when do_fcd is off */
+    double *sim_states;        /* may be NULL when ext_out is off */
+    uint8_t *global_bools;
+    int32_t *global_ints;
+    double *noise;             /* only written when noise_out */
+    int32_t *shuffled_nodes;
+    int32_t *shuffled_ts;
+    double init_time;          /* seconds, written by the library */
+    double run_time;           /* seconds, written by the library */
+} cbnm_outputs;
+
+/* Device timings of the last run, in milliseconds (CUDA events). */
+typedef struct cbnm_timing {
+    double integrate_ms;       /* the integrator kernel (neural model + BOLD) */
+    double fc_ms;              /* FC / FCD kernels */
+    double h2d_ms;             /* host-to-device copies of the inputs */
+    double d2h_ms;             /* device-to-host copies of the outputs */
+    double total_ms;
+    int64_t h2d_bytes;
+    int64_t d2h_bytes;
+    int kernel_launches;       /* kernels this library launched in the run */
+} cbnm_timing;
+
+/* core.cpp:147-155 -- resets the Balloon-Windkessel constants to their defaults. */
+int cbnm_init(void);
+
+/* core.cpp:157-192 -- sets k1, k2, k3 or V_0 of the Balloon-Windkessel model. */
+int cbnm_set_const(const char *key, double value);
+
+/* Sizes of every output of run_simulations for these arguments (core.cpp:336-349). */
+int cbnm_query_sizes(const cbnm_run_args *args, cbnm_sizes *sizes);
+
+/* core.cpp:194-493 (run_simulations) -- host buffers in, host buffers out.
+ * Extra model_config key understood by this library: "precision" = "fp64"
+ * (default; matches the reference's double build) or "fp32" (FP32 node state,
+ * tensor-core coupling; FP64 Balloon-Windkessel and FC/FCD denominators). */
+int cbnm_run_simulations(const cbnm_run_args *args, cbnm_outputs *out);
+
+/* Same as cbnm_run_simulations, but every array pointer in args and out is a
+ * device pointer on the current CUDA device (inputs already resident in HBM).
+ * No reference counterpart: it is the device-resident form of core.cpp:194-493. */
+int cbnm_run_simulations_device(const cbnm_run_args *args, cbnm_outputs *out);
+
+/* Timings of the last cbnm_run_simulations[_device] call. */
+int cbnm_last_timing(cbnm_timing *timing);
+
+/* Drops the cached session (device buffers and noise); core.cpp keeps it for
+ * the process lifetime, this lets a host free the memory early. */
+int cbnm_reset(void);
+
+/* Human-readable description of the last error (empty if none). */
+const char *cbnm_last_error(void);
+
+/* Goodness-of-fit seam (src/cubnm/utils.py:416-507 fc_corr_device and
+ * :306-414 fcd_ks_device; src/cubnm/sim/base.py:1165-1189 for fc_diff and
+ * fc_normec).  Host arrays; all outputs [n_sims].
+ *   fc_corr  : Pearson r between each sim_fc row and emp_fc
+ *   fc_diff  : |mean(sim_fc) - mean(emp_fc)|
+ *   fc_normec: ||sim_fc - emp_fc||_2 / (2 sqrt(n_pairs))
+ *   fcd_ks   : two-sample Kolmogorov-Smirnov distance between each sim_fcd row and emp_fcd
+ * Any output pointer may be NULL to skip that term. */
+int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc,
+             const double *sim_fcd, int n_window_pairs, const double *emp_fcd, int n_emp_fcd,
+             double *fc_corr, double *fc_diff, double *fc_normec, double *fcd_ks);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUBNM_B200_H */
