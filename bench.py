@@ -1,0 +1,340 @@
+"""Benchmark: rWW simulations x simulated seconds per wall second.
+
+Workload (the reference's headline case): reduced Wong-Wang, 100 nodes,
+32,768 simulations, 60 s each, dt 0.1 ms, BOLD TR 1 s, FC + FCD (window 10,
+step 2), no FIC, no delay; G, w_p, J_N drawn uniformly from the grid ranges
+G in [0.001, 10], w_p in [0, 2], J_N in [0.001, 0.5]; synthetic SC (symmetric,
+30% density, lognormal weights, mean row sum 1); noise from the seeded
+generator.  One "step" = one run of all simulations (integration + BOLD +
+FC/FCD).  The BOLD output alone (1.57 GB) is larger than L2, so no L2 flush is
+needed between steps.
+
+value : FP32 / tensor-core path, inputs resident in HBM (device C-ABI entry).
+e2e   : the same through the host C-ABI entry (cbnm_run_simulations with host
+        buffers: parameters and SC copied in, BOLD/FC/FCD/states copied out)
+        plus the GOF scoring call, timed on the host.
+fp64  : the FP64 reference-precision path, measured on a 4,736-simulation
+        subset (a full GPU wave), for the precision/speed comparison.
+
+--impl reference times the reference's own CPU algorithm (the oracle
+restatement, OpenMP over simulations, all host threads) on a bounded sample.
+Under torchrun every rank integrates its own 32,768 simulations (weak scaling;
+simulations are independent, no collective on the data path).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+N_SIMS = 32768
+NODES = 100
+DURATION_S = 60
+WORKLOAD = f"rWW {NODES} nodes, {N_SIMS} sims, {DURATION_S} s, dt 0.1 ms, TR 1 s, FC+FCD w10/s2"
+METRIC = "rWW sims x sim-s per wall-s (100 nodes, 32k sims)"
+UNIT = "sims*sim-s/s"
+
+
+def workload_args(n_sims, duration_s, precision, seed):
+    import cases
+    rng = np.random.default_rng(1000 + seed)
+    G = rng.uniform(0.001, 10, n_sims)
+    wp = rng.uniform(0, 2, n_sims)
+    jn = rng.uniform(0.001, 0.5, n_sims)
+    # the headline case removes 30 s of BOLD before FC; short profiling runs keep 3/4 of it
+    remove = 30 if duration_s >= 60 else duration_s // 4
+    window = 10 if duration_s - remove > 12 else 2
+    return list(cases.synthetic_args("rWW", N=n_sims, nodes=NODES, duration_s=duration_s, seed=0, G=G, w_p=wp,
+                                     J_N=jn, precision=precision, window_size=window, window_step=2,
+                                     bold_remove_s=remove))
+
+
+class Clocks:
+    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, name in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(name)
+            except Exception:
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def device_buffers(torch, args, sizes, dev):
+    """Inputs copied to HBM once; outputs allocated on the device."""
+    from cubnm_b200 import _abi
+    t = {}
+    t["sc"] = torch.from_numpy(np.ascontiguousarray(args[1])).to(dev)
+    t["sc_idx"] = torch.from_numpy(np.ascontiguousarray(args[2], dtype=np.int32)).to(dev)
+    t["dist"] = torch.from_numpy(np.ascontiguousarray(args[3])).to(dev)
+    t["g"] = torch.from_numpy(np.ascontiguousarray(args[4])).to(dev)
+    t["r"] = torch.from_numpy(np.ascontiguousarray(args[5])).to(dev)
+    t["v"] = torch.from_numpy(np.ascontiguousarray(args[6])).to(dev)
+    N, n = args[14], args[15]
+    t["bold"] = torch.empty((N, sizes.bold_len * n), dtype=torch.float64, device=dev)
+    t["fc"] = torch.empty((N, sizes.n_pairs), dtype=torch.float64, device=dev)
+    t["fcd"] = torch.empty((N, max(1, sizes.n_window_pairs)), dtype=torch.float64, device=dev)
+    t["states"] = torch.empty((sizes.n_state_vars, N, n), dtype=torch.float64, device=dev)
+    t["gb"] = torch.empty((max(1, sizes.n_global_out_bool), N), dtype=torch.uint8, device=dev)
+    t["gi"] = torch.empty((max(1, sizes.n_global_out_int), N), dtype=torch.int32, device=dev)
+    dp = lambda x: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+    p = _abi.Prepared(*args)
+    a = p.args
+    a.sc = dp(t["sc"])
+    a.sc_indices = C.cast(C.c_void_p(t["sc_idx"].data_ptr()), C.POINTER(C.c_int32))
+    a.sc_dist = dp(t["dist"])
+    a.global_params = dp(t["g"])
+    a.regional_params = dp(t["r"])
+    a.v_list = dp(t["v"])
+    o = _abi.Outputs(dp(t["bold"]), dp(t["fc"]), dp(t["fcd"]), dp(t["states"]),
+                     C.cast(C.c_void_p(t["gb"].data_ptr()), C.POINTER(C.c_uint8)),
+                     C.cast(C.c_void_p(t["gi"].data_ptr()), C.POINTER(C.c_int32)), None, None, None, 0.0, 0.0)
+    return t, p, o
+
+
+def run_ours(opts, rank, world, local_rank):
+    import torch
+    from cubnm_b200 import _abi, core, utils
+    from cubnm_b200._lib import lib, check
+    import cases
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = lib()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n_sims = opts.sims
+    args = workload_args(n_sims, opts.duration, opts.precision, seed=rank)
+    sizes = _abi.Sizes()
+    check(L.cbnm_query_sizes(C.byref(_abi.Prepared(*args).args), C.byref(sizes)))
+    bufs, prep, outs = device_buffers(torch, args, sizes, dev)
+    st = torch.cuda.current_stream()
+
+    def device_step():
+        check(L.cbnm_run_simulations_device(C.byref(prep.args), C.byref(outs)))
+        return core.last_timing()
+
+    # warm-up (first call also generates the noise segment: session init)
+    for _ in range(opts.warmup):
+        device_step()
+    clocks = Clocks(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]) if world == 1 else local_rank)
+    clocks.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    integ_ms, fc_ms, launches = [], [], 0
+    for _ in range(opts.steps):
+        tm = device_step()
+        integ_ms.append(tm["integrate_ms"])
+        fc_ms.append(tm["fc_ms"])
+        launches += tm["kernel_launches"]
+    e1.record(st)
+    barrier()
+    ck = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / opts.steps)
+    value = world * n_sims * opts.duration / (ms / 1e3)
+
+    # end to end through the host C ABI (host buffers; copies inside the timed region) + GOF scoring
+    emp = cases.synthetic_emp_bold(NODES, opts.duration, 7)
+    emp_fc = utils.calculate_fc(emp)
+    emp_fcd = utils.calculate_fcd(emp, 10 if opts.duration >= 16 else 2, 2)
+    host_args = [a.copy() if isinstance(a, np.ndarray) else a for a in args]
+    core.run_simulations(*host_args)  # warm the host path
+    e2e_steps = max(1, opts.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(e2e_steps):
+        out = core.run_simulations(*host_args)
+        tm = core.last_timing()
+        h2d += tm["h2d_bytes"]
+        d2h += tm["d2h_bytes"]
+        g = utils.gof(out["sim_fc_trils"], emp_fc, out["sim_fcd_trils"], emp_fcd)
+        launches_e2e = tm["kernel_launches"]
+        assert np.isfinite(g["fc_corr"]).mean() > 0.5
+    barrier()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+    e2e_value = world * n_sims * opts.duration / e2e_s
+
+    # FP64 reference-precision path on one full wave, same metric
+    fp64 = None
+    if not opts.skip_fp64:
+        n64 = min(n_sims, 4736)
+        a64 = workload_args(n64, opts.duration, "fp64", seed=rank)
+        core.run_simulations(*a64)
+        t64 = core.last_timing()
+        fp32_sub = workload_args(n64, opts.duration, opts.precision, seed=rank)
+        core.run_simulations(*fp32_sub)
+        t32 = core.last_timing()
+        fp64 = {"value": n64 * opts.duration / ((t64["integrate_ms"] + t64["fc_ms"]) / 1e3),
+                "fp32_same_subset": n64 * opts.duration / ((t32["integrate_ms"] + t32["fc_ms"]) / 1e3),
+                "sims": n64, "unit": UNIT}
+
+    # roofline of the dominant kernel (the integrator): coupling on the tensor pipe
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak_tf = peaks.get("bf16_tflops_sustained") or 1400.0
+    node_steps = n_sims * NODES * (opts.duration * 1000 / 0.1)
+    integ = float(np.mean(integ_ms)) / 1e3
+    useful = 2.0 * NODES * node_steps  # coupling flops (2 n per node-step)
+    issued = 3 * 2.0 * 128 * (((NODES + 15) // 16) * 16) * (n_sims * 1.0) * (opts.duration * 1e4)  # BF16x3 MMA work
+    roof = {"bound": "tensor", "achieved": useful / integ / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": useful / integ / 1e12 / peak_tf,
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else "fallback",
+            "mma_issued_tflops": issued / integ / 1e12,
+            "traffic": opts.traffic, "kernel": "k_integrate_tc<RWW32>", "kernel_ms": integ * 1e3,
+            "note": "integrator is bound by the FP32/MUFU elementwise update, not the tensor pipe; see profiles/"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": opts.steps,
+        "warmup": opts.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (BF16x3 tensor-core coupling, FP64 Balloon-Windkessel and FC/FCD)",
+        "data": "synthetic (seeded SC, parameters and noise)",
+        "config": {"workload": WORKLOAD, "sims_per_gpu": n_sims, "nodes": NODES, "duration_s": opts.duration,
+                   "precision": opts.precision, "parallelism": f"independent sims x{world}",
+                   "l2": "inputs/outputs larger than L2 (BOLD 1.57 GB per step); no flush"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
+                "d2h_bytes_per_step": d2h // e2e_steps, "includes": "H2D params/SC, kernels, D2H outputs, GOF"},
+        "gpu_launches": launches,
+        "kernel_ms": {"integrate": float(np.mean(integ_ms)), "fc_fcd": float(np.mean(fc_ms))},
+        "fp64_path": fp64,
+        "roofline": roof,
+        "clocks": ck,
+    }
+    if not opts.skip_cpu and rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(opts)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(opts, sample=None):
+    """The reference's CPU algorithm (oracle restatement, OpenMP over sims, all host threads)."""
+    from oracle import oracle
+    threads = oracle.num_threads()
+    sample = sample or max(16, 2 * threads)
+    args = workload_args(sample, opts.duration, "fp64", seed=0)
+    t0 = time.perf_counter()
+    oracle.run_simulations(*args)
+    el = time.perf_counter() - t0
+    return {"value": sample * opts.duration / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample} sims x {opts.duration} s of the workload (same params distribution), "
+                      f"{el:.1f} s wall"}
+
+
+def run_reference(opts, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle
+    threads = oracle.num_threads()
+    sample = max(16, 2 * threads)
+    args = workload_args(sample, opts.duration, "fp64", seed=0)
+    for _ in range(max(0, min(opts.warmup, 1))):
+        oracle.run_simulations(*[a.copy() if isinstance(a, np.ndarray) else a for a in args])
+    t0 = time.perf_counter()
+    for _ in range(opts.steps):
+        oracle.run_simulations(*[a.copy() if isinstance(a, np.ndarray) else a for a in args])
+    el = (time.perf_counter() - t0) / opts.steps
+    value = sample * opts.duration / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": opts.steps, "warmup": opts.warmup, "ms_per_step": el * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_sims_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample} sims x {opts.duration} s per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--sims", type=int, default=N_SIMS)
+    ap.add_argument("--duration", type=int, default=DURATION_S)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per integrator launch")
+    opts = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:  # one GPU per process
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    if opts.impl == "reference":
+        run_reference(opts, rank, world)
+    else:
+        run_ours(opts, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+// Internal interface between the host session (session.cpp) and the kernels.
+// Not part of the public C ABI (include/cubnm_b200.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cbnm {
+
+enum ModelId { MODEL_RWW = 0, MODEL_WC = 1, MODEL_JR = 2, MODEL_KURAMOTO = 3, MODEL_RWWEX = 4 };
+
+// Balloon-Windkessel constants (reference: src/ext/models/bw.cpp:4-22).
+struct BWConst {
+    double dt, rho, alpha, tau, y, kappa, V_0, k1, k2, k3;
+    double ialpha, itau, oneminrho, dt_itau, V_0_k1, V_0_k2, V_0_k3;
+};
+
+// Model constants, computed on the host exactly as the reference's
+// init_constants(dt) does (src/ext/models/<model>.cpp).
+struct RWWK {
+    double dt, sqrt_dt, a_E, b_E, d_E, a_I, b_I, d_I, w_II, w_E__I_0, w_I__I_0, b_a_ratio_E;
+    double dt_itau_E, dt_gamma_E, dt_itau_I, dt_gamma_I;
+    // analytical-FIC constants (rww.cpp:42-53)
+    double I_0, w_E, w_I, I_ext, tau_I_s, gamma_I_s, I_E_ss, S_E_ss;
+};
+struct WCK { double dt, sqrt_dt, itau_E, itau_I, a_E, a_I, mu_E, mu_I; };
+struct JRK { double dt, sqrt_dt, A, B, a, b, v0, nu_max, r, mu, cmin, cmax, midpoint, a_sq, b_sq; };
+struct KurK { double dt, sqrt_dt, twopi; };
+struct RWWExK { double dt, sqrt_dt, J_N, a, b, d, dt_itau, dt_gamma; };
+union ModelK {
+    RWWK rww;
+    WCK wc;
+    JRK jr;
+    KurK kur;
+    RWWExK rwwex;
+};
+
+// Static description of each model (include/cubnm/models/<model>.hpp).
+struct ModelDesc {
+    const char *name;
+    int id, n_state, n_inter, n_noise, n_global, n_regional, conn_idx, bold_idx, n_gout_bool, n_gout_int;
+    bool osc, post_bw, modifies_params;
+};
+const ModelDesc *find_model(const char *name);
+
+// Arguments of the integrator kernels (one persistent time loop per simulation).
+struct IntegrateArgs {
+    int nodes, n_sims, bw_it, inner_it, bold_tr_iters, states_sampling_iters, n_states_samples_remove;
+    int noise_bw_it, bold_len, states_len, ext_out, states_ts;
+    const double *sc;            // [n_scs][nodes*nodes] (FP64 kernel)
+    const float *sc_f32;         // [n_scs][nodes*nodes] (FP32 kernel)
+    const int *sc_idx;           // [n_sims]
+    const double *gparams;       // [n_global][n_sims]
+    const double *rparams;       // [n_regional][n_sims*nodes]
+    double *rparams_out;         // wIE write-back (rWW FIC)
+    const double *noise;         // [noise_size]
+    const float *noise_f32;      // [noise_size] (FP32 kernel)
+    const int *sh_nodes;         // [repeats][nodes]
+    const int *sh_ts;            // [repeats][noise_bw_it]
+    int has_delay;
+    const int *delay;            // [n_tables][nodes*nodes] integration steps, row = source
+    const int *delay_idx;        // [n_sims] table of each simulation
+    const int *max_delay;        // [n_sims]
+    const long long *hist_off;   // [n_sims] offset of each simulation's ring buffer
+    double *hist;                // ring buffers (FP64 kernel)
+    float *hist_f32;             // ring buffers (FP32 kernel)
+    double *bold;                // [n_sims][bold_len*nodes]
+    double *states;              // [n_state][n_sims][nodes or nodes*states_len]
+    unsigned char *gbools;       // [n_gout_bool][n_sims]
+    int *gints;                  // [n_gout_int][n_sims]
+    int do_fic, max_fic_trials, I_start, I_end, I_dur;
+    double init_delta;
+    BWConst bw;
+    ModelK K;
+    int sim_begin;               // first simulation of this launch (FP64 kernel)
+    int n_regional;              // regional parameters of the model
+    const int *tiles;            // FP32 kernel: [n_tiles][1 + fp32_tile_sims()] = SC index, then simulation ids (-1 = empty)
+    int n_tiles;
+    int *status;                 // device status word (0 = ok)
+};
+
+// FC / FCD (reference: src/ext/fc.cu, src/ext/fc.cpp).
+struct FcArgs {
+    int nodes, bold_len, n_vols_remove, n_pairs, n_windows, n_window_pairs;
+    int max_T;                   // longest volume range of the static FC and the windows
+    int sim_begin, sim_count;
+    const int *w_start, *w_end;  // [n_windows] inclusive volume ranges
+    const int *pair_i, *pair_j;  // [n_pairs] node pair of each FC entry
+    const double *bold;          // [n_sims][bold_len*nodes]
+    double *fc;                  // [n_sims][n_pairs]
+    double *fcd;                 // [n_sims][n_window_pairs]
+    double *wfc;                 // scratch [sim_count][n_windows][n_pairs]
+    double *wstat;               // scratch [sim_count][n_windows][2] (mean, ssd)
+};
+
+// Goodness of fit.
+struct GofArgs {
+    int n_sims, n_pairs, n_wp, n_emp_fcd;
+    const double *sim_fc, *emp_fc, *sim_fcd, *emp_fcd_sorted;
+    double emp_fc_mean, emp_fc_ssd;  // mean and sqrt(sum (x - mean)^2) of emp_fc
+    double *fc_corr, *fc_diff, *fc_normec, *fcd_ks;
+};
+
+// launchers (return cudaGetLastError() of the launch)
+cudaError_t launch_integrate_fp64(int model, const IntegrateArgs &a, cudaStream_t st);
+cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
+bool fp32_supported(int model, int nodes, bool has_delay);
+int fp32_tile_sims();
+cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
+cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
+size_t gof_ks_smem_limit();
+
+}  // namespace cbnm

@@ -1,0 +1,972 @@
+// Host side of the cubnm_b200 C ABI (include/cubnm_b200.h).
+//
+// Replaces the reference's CPython boundary and session logic:
+//   run_simulations / init / set_const   src/ext/core.cpp:147-504
+//   model object sizes and config        include/cubnm/models/base.hpp:51-124, 271-297
+//   session init (noise, windows, pairs) src/ext/bnm.cu:990-1265
+//   run (params, delays, kernels, copy)  src/ext/bnm.cu:507-988
+//   rWW analytical FIC                   src/ext/models/rww.cpp:73-146, rww_fic.cpp:62-231
+// Design differences: plain device allocations (no managed memory), one
+// stream, CUDA-event timings, status codes instead of exceptions, a cached
+// session keyed on everything that changes the noise (as bnm.cu:1207-1215).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cubnm_b200.h"
+#include "engine.h"
+
+namespace cbnm {
+
+// ---------------------------------------------------------------- models
+static const ModelDesc kModels[] = {
+    // name, id, states, inter, noise, global, regional, conn, bold, gout_bool, gout_int, osc, post_bw, modifies
+    {"rWW", MODEL_RWW, 6, 7, 2, 1, 4, 4, 4, 2, 1, false, true, true},
+    {"WC", MODEL_WC, 2, 4, 2, 1, 8, 0, 0, 0, 0, false, false, false},
+    {"JR", MODEL_JR, 8, 9, 1, 1, 6, 7, 6, 0, 0, false, false, false},
+    {"Kuramoto", MODEL_KURAMOTO, 1, 1, 1, 1, 3, 0, 0, 0, 0, true, false, false},
+    {"rWWEx", MODEL_RWWEX, 3, 2, 1, 1, 3, 2, 2, 0, 0, false, false, false},
+};
+
+const ModelDesc *find_model(const char *name) {
+    if (!name) return nullptr;
+    for (const auto &m : kModels)
+        if (std::strcmp(m.name, name) == 0) return &m;
+    return nullptr;
+}
+
+struct Err : std::runtime_error {
+    int code;
+    Err(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: ") + cudaGetErrorString(e_) + " at " +    \
+                                         __FILE__ + ":" + std::to_string(__LINE__));                    \
+    } while (0)
+
+// ---------------------------------------------------------------- constants
+static BWConst bw_defaults(double dt_s) {  // bw.cpp:4-22
+    BWConst c;
+    c.dt = dt_s; c.rho = 0.34; c.alpha = 0.32; c.tau = 0.98; c.y = 1.0 / 0.41; c.kappa = 1.0 / 0.65;
+    c.V_0 = 0.02 * 100; c.k1 = 7 * c.rho; c.k2 = 2.0; c.k3 = 2 * c.rho - 0.2;
+    c.ialpha = 1.0 / c.alpha; c.itau = 1.0 / c.tau; c.oneminrho = (1.0 - c.rho); c.dt_itau = c.dt * c.itau;
+    c.V_0_k1 = c.V_0 * c.k1; c.V_0_k2 = c.V_0 * c.k2; c.V_0_k3 = c.V_0 * c.k3;
+    return c;
+}
+static BWConst g_bw = bw_defaults(0.001);
+static std::string g_err;
+
+static ModelK make_constants(int model, double dt) {
+    ModelK K;
+    std::memset(&K, 0, sizeof(K));
+    switch (model) {
+        case MODEL_RWW: {  // rww.cpp:8-53
+            RWWK &m = K.rww;
+            m.dt = dt; m.sqrt_dt = std::sqrt(m.dt);
+            m.a_E = 310; m.b_E = 125; m.d_E = 0.16; m.a_I = 615; m.b_I = 177; m.d_I = 0.087;
+            const double gamma_E = (double)0.641 / (double)1000.0, gamma_I = (double)1.0 / (double)1000.0;
+            const double tau_E = 100, tau_I = 10;
+            m.I_0 = 0.382; m.w_E = 1.0; m.w_I = 0.7; m.w_II = 1.0; m.I_ext = 0.0;
+            m.w_E__I_0 = m.w_E * m.I_0; m.w_I__I_0 = m.w_I * m.I_0; m.b_a_ratio_E = m.b_E / m.a_E;
+            const double itau_E = 1.0 / tau_E, itau_I = 1.0 / tau_I;
+            m.dt_itau_E = m.dt * itau_E; m.dt_gamma_E = m.dt * gamma_E;
+            m.dt_itau_I = m.dt * itau_I; m.dt_gamma_I = m.dt * gamma_I;
+            m.tau_I_s = 0.01; m.gamma_I_s = 1.0; m.I_E_ss = 0.3773805650; m.S_E_ss = 0.1647572075;
+            break;
+        }
+        case MODEL_WC: {  // wc.cpp:14-25
+            WCK &m = K.wc;
+            m.dt = dt; m.sqrt_dt = std::sqrt(m.dt);
+            const double tau_E = 2.5, tau_I = 3.75;
+            m.itau_E = 1.0 / tau_E; m.itau_I = 1.0 / tau_I; m.a_E = 1.5; m.a_I = 1.5; m.mu_E = 3.0; m.mu_I = 3.0;
+            break;
+        }
+        case MODEL_JR: {  // jr.cpp:14-30
+            JRK &m = K.jr;
+            m.dt = dt; m.sqrt_dt = std::sqrt(m.dt); m.A = 3.25; m.B = 22.0; m.a = 0.1; m.b = 0.05; m.v0 = 6.0;
+            m.nu_max = 0.0025; m.r = 0.56; m.mu = 0.22; m.cmin = 0.0; m.cmax = 0.005; m.midpoint = 6.0;
+            m.a_sq = std::pow(m.a, 2); m.b_sq = std::pow(m.b, 2);
+            break;
+        }
+        case MODEL_KURAMOTO: {  // kuramoto.cpp:14-18
+            KurK &m = K.kur;
+            m.dt = dt; m.sqrt_dt = std::sqrt(m.dt); m.twopi = 2.0 * M_PI;
+            break;
+        }
+        case MODEL_RWWEX: {  // rwwex.cpp:14-26
+            RWWExK &m = K.rwwex;
+            m.dt = dt; m.sqrt_dt = std::sqrt(m.dt); m.J_N = 0.2609; m.a = 270; m.b = 108; m.d = 0.154;
+            const double gamma = (double)0.641 / (double)1000.0, tau = 100, itau = 1.0 / tau;
+            m.dt_itau = m.dt * itau; m.dt_gamma = m.dt * gamma;
+            break;
+        }
+    }
+    return K;
+}
+
+// ---------------------------------------------------------------- config
+struct Cfg {
+    bool verbose = false, do_fc = true, do_fcd = true;
+    int bold_remove_s = 30;
+    bool exc_inter = true;
+    int window_size = 10, window_step = 2;
+    bool drop_edges = true, ext_out = true, states_ts = false;
+    int noise_time_steps = 30000;
+    bool do_fic = true;
+    int max_fic_trials = 0;
+    int I_start = 1000, I_end = 10000, I_dur = 10000 - 1000 + 1;
+    double init_delta = 0.02;
+    bool fp32 = false;
+    int nodes = 0, n_sims = 0, time_steps = 0, bold_tr = 0, states_sampling = 0, sim_seed = 0;
+    double dt = 0.1, bw_dt = 0.001;
+    int bold_len = 0, bold_tr_iters = 0, states_len = 0, states_sampling_iters = 0, bw_it = 0, inner_it = 0;
+    int n_vols_remove = 0, n_states_samples_remove = 0, corr_len = 0;
+    int n_pairs = 0, n_windows = 0, n_window_pairs = 0;
+    std::vector<int> w_start, w_end;
+    int noise_bw_it = 0, noise_repeats = 0;
+    int64_t noise_size = 0;
+};
+
+static int to_int(const std::string &k, const std::string &v) {
+    try {
+        size_t pos = 0;
+        int x = std::stoi(v, &pos);
+        return x;
+    } catch (...) {
+        throw Err(CBNM_ERR_CONFIG, "invalid integer for config key '" + k + "': '" + v + "'");
+    }
+}
+
+static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
+    c.nodes = a->nodes; c.n_sims = a->n_sims; c.time_steps = a->time_steps; c.bold_tr = a->bold_tr;
+    c.states_sampling = a->states_sampling; c.sim_seed = a->sim_seed; c.dt = a->dt; c.bw_dt = a->bw_dt / 1000.0;
+    c.ext_out = a->ext_out != 0; c.states_ts = a->states_ts != 0;
+    for (int i = 0; i < a->n_config; ++i) {  // base.hpp:271-297, rww.cpp:54-71
+        if (!a->config_keys || !a->config_values || !a->config_keys[i] || !a->config_values[i])
+            throw Err(CBNM_ERR_ARG, "null config key or value");
+        const std::string k = a->config_keys[i], v = a->config_values[i];
+        if (k == "verbose") c.verbose = to_int(k, v) != 0;
+        else if (k == "do_fc") c.do_fc = to_int(k, v) != 0;
+        else if (k == "do_fcd") c.do_fcd = to_int(k, v) != 0;
+        else if (k == "bold_remove_s") c.bold_remove_s = to_int(k, v);
+        else if (k == "exc_interhemispheric") c.exc_inter = to_int(k, v) != 0;
+        else if (k == "window_size") c.window_size = to_int(k, v);
+        else if (k == "window_step") c.window_step = to_int(k, v);
+        else if (k == "drop_edges") c.drop_edges = to_int(k, v) != 0;
+        else if (k == "noise_time_steps") c.noise_time_steps = to_int(k, v);
+        else if (k == "precision") {
+            if (v == "fp32") c.fp32 = true;
+            else if (v == "fp64") c.fp32 = false;
+            else throw Err(CBNM_ERR_CONFIG, "precision must be 'fp64' or 'fp32', got '" + v + "'");
+        }
+        if (md.id == MODEL_RWW) {
+            if (k == "do_fic") c.do_fic = to_int(k, v) != 0;
+            else if (k == "max_fic_trials") c.max_fic_trials = to_int(k, v);
+            else if (k == "I_SAMPLING_START") c.I_start = (int)((to_int(k, v) / 1000) / c.bw_dt);
+            else if (k == "I_SAMPLING_END") c.I_end = (int)((to_int(k, v) / 1000) / c.bw_dt);
+            else if (k == "init_delta") c.init_delta = std::stod(v);
+        }
+    }
+    c.I_dur = c.I_end - c.I_start + 1;
+    if (md.id != MODEL_RWW) c.do_fic = false;
+    if (c.nodes <= 0 || c.n_sims <= 0) throw Err(CBNM_ERR_ARG, "nodes and N_SIMS must be positive");
+    if (c.bold_tr <= 0 || c.states_sampling <= 0 || c.time_steps <= 0 || c.dt <= 0 || c.bw_dt <= 0)
+        throw Err(CBNM_ERR_ARG, "time_steps, BOLD_TR, states_sampling, dt and bw_dt must be positive");
+    // base.hpp:51-68 (truncating conversions kept)
+    c.bold_len = c.time_steps / c.bold_tr;
+    c.bold_tr_iters = (int)(((double)c.bold_tr / 1000.0) / c.bw_dt);
+    c.states_len = c.time_steps / c.states_sampling;
+    c.states_sampling_iters = (int)(((double)c.states_sampling / 1000.0) / c.bw_dt);
+    c.bw_it = (int)(((double)c.time_steps / 1000.0) / c.bw_dt);
+    c.inner_it = (int)((c.bw_dt * 1000) / c.dt);
+    if (c.bold_tr_iters <= 0 || c.states_sampling_iters <= 0 || c.bw_it <= 0 || c.inner_it <= 0)
+        throw Err(CBNM_ERR_ARG, "BOLD_TR, states_sampling and duration must be multiples of bw_dt, bw_dt of dt");
+    c.n_states_samples_remove = c.bold_remove_s * 1000 / c.states_sampling;
+    if (c.do_fc) {  // bnm.cu:1078-1182
+        c.n_vols_remove = c.bold_remove_s * 1000 / c.bold_tr;
+        c.corr_len = c.bold_len - c.n_vols_remove;
+        if (c.corr_len < 2)
+            throw Err(CBNM_ERR_CONFIG, "Number of BOLD volumes (after removing " + std::to_string(c.n_vols_remove) +
+                                           " initial volumes) is " + std::to_string(c.corr_len) +
+                                           " which is too low for FC calculations");
+        c.n_pairs = c.nodes * (c.nodes - 1) / 2;
+        if (c.exc_inter) {
+            if (c.nodes % 2 != 0) throw Err(CBNM_ERR_CONFIG, "exc_interhemispheric is set but number of nodes is not even");
+            c.n_pairs -= (c.nodes / 2) * (c.nodes / 2);
+        }
+        if (c.do_fcd) {  // utils.cpp:21-52
+            int first = c.drop_edges ? c.window_size / 2 : 0;
+            int last = c.drop_edges ? c.corr_len - 1 - c.window_size / 2 : c.corr_len - 1;
+            first += c.n_vols_remove;
+            last += c.n_vols_remove;
+            if (c.window_step <= 0) throw Err(CBNM_ERR_CONFIG, "window_step must be positive");
+            for (int ctr = first; ctr <= last; ctr += c.window_step) {
+                int s = std::max(0, ctr - c.window_size / 2);
+                int e = std::min(c.bold_len - 1, ctr + c.window_size / 2);
+                c.w_start.push_back(s);
+                c.w_end.push_back(e);
+            }
+            c.n_windows = (int)c.w_start.size();
+            if (c.n_windows == 0) throw Err(CBNM_ERR_CONFIG, "Number of dynamic FC windows is 0");
+            c.n_window_pairs = c.n_windows * (c.n_windows - 1) / 2;
+        }
+    } else {
+        c.do_fcd = false;
+    }
+    c.noise_bw_it = (int)(((double)(c.noise_time_steps) / 1000.0) / c.bw_dt);  // bnm.cu:1229-1231
+    if (c.noise_bw_it <= 0) throw Err(CBNM_ERR_CONFIG, "noise_time_steps must cover at least one bw_dt");
+    c.noise_repeats = (int)std::ceil((double)(c.bw_it) / (double)(c.noise_bw_it));
+    c.noise_size = (int64_t)c.nodes * c.noise_bw_it * c.inner_it * md.n_noise;
+}
+
+// ---------------------------------------------------------------- noise
+// bnm.cu:1240-1256 + utils.cpp:74-95.  The values come from std::mt19937 and
+// libstdc++'s std::normal_distribution<double>; the node and time shuffles are
+// restated explicitly: the bounded draw is the division-based rejection method
+// and two swap positions come from one draw in [0, (i+1)(i+2)), which is what
+// the libstdc++ that produced the reference's stored outputs does.
+static uint64_t bounded_draw(std::mt19937 &g, uint64_t range_max) {
+    const uint64_t urng_range = 0xffffffffULL;
+    const uint64_t span = range_max + 1, scaling = urng_range / span, past = span * scaling;
+    uint64_t r;
+    do { r = (uint64_t)g(); } while (r >= past);
+    return r / scaling;
+}
+static void shuffle_positions(std::vector<int> &v, std::mt19937 &g) {
+    const size_t n = v.size();
+    if (n < 2) return;
+    size_t i = 1;
+    if (n % 2 == 0) { std::swap(v[i], v[bounded_draw(g, 1)]); ++i; }
+    while (i != n) {
+        const uint64_t b0 = i + 1, b1 = i + 2, x = bounded_draw(g, b0 * b1 - 1);
+        std::swap(v[i], v[x / b1]); ++i;
+        std::swap(v[i], v[x % b1]); ++i;
+    }
+}
+
+// ---------------------------------------------------------------- device buffers
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    void *ensure(size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        if (bytes > cap) {
+            if (p) CK(cudaFree(p));
+            p = nullptr;
+            cap = 0;
+            CK(cudaMalloc(&p, bytes));
+            cap = bytes;
+        }
+        return p;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() { return static_cast<T *>(p); }
+};
+
+struct Session {
+    bool ready = false;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8];
+    // noise cache (bnm.cu:1207-1215 key)
+    bool noise_valid = false, noise_f32_valid = false;
+    int k_seed = 0, k_time = 0, k_nodes = 0, k_nts = 0, k_nnoise = 0;
+    double k_bwdt = 0, k_dt = 0;
+    std::vector<double> noise;
+    std::vector<int> sh_nodes, sh_ts;
+    DBuf d_noise, d_noise_f32, d_sh_nodes, d_sh_ts;
+    // run buffers
+    DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
+    DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
+    DBuf d_tiles;
+    // gof
+    DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
+    cbnm_timing timing{};
+    ~Session() {}
+};
+static Session *g_sess = nullptr;
+
+static Session &session() {
+    if (!g_sess) g_sess = new Session();
+    Session &S = *g_sess;
+    if (!S.ready) {
+        int ndev = 0;
+        cudaError_t e = cudaGetDeviceCount(&ndev);
+        if (e != cudaSuccess || ndev == 0)
+            throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: no CUDA device available (") + cudaGetErrorString(e) + ")");
+        CK(cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking));
+        for (auto &ev : S.ev) CK(cudaEventCreate(&ev));
+        S.ready = true;
+    }
+    return S;
+}
+
+static void release_session() {
+    if (!g_sess) return;
+    Session &S = *g_sess;
+    if (S.ready) {
+        cudaStreamSynchronize(S.st);
+        for (DBuf *b : {&S.d_noise, &S.d_noise_f32, &S.d_sh_nodes, &S.d_sh_ts, &S.d_sc, &S.d_sc_f32, &S.d_sc_idx,
+                        &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
+                        &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
+                        &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
+                        &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
+            b->release();
+        for (auto &ev : S.ev) cudaEventDestroy(ev);
+        cudaStreamDestroy(S.st);
+    }
+    delete g_sess;
+    g_sess = nullptr;
+}
+
+static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool force) {
+    const bool same = S.noise_valid && S.k_seed == c.sim_seed && S.k_time == c.time_steps && S.k_nodes == c.nodes &&
+                      S.k_nts == c.noise_time_steps && S.k_nnoise == md.n_noise && S.k_bwdt == c.bw_dt &&
+                      S.k_dt == c.dt;
+    if (!same || force) {
+        std::mt19937 gen(c.sim_seed);
+        std::normal_distribution<double> nd(0, 1);
+        S.noise.resize((size_t)c.noise_size);
+        for (int64_t i = 0; i < c.noise_size; ++i) S.noise[i] = nd(gen);
+        std::vector<int> idx(c.nodes);
+        S.sh_nodes.resize((size_t)c.noise_repeats * c.nodes);
+        std::iota(idx.begin(), idx.end(), 0);
+        for (int r = 0; r < c.noise_repeats; ++r) {
+            shuffle_positions(idx, gen);
+            std::copy(idx.begin(), idx.end(), S.sh_nodes.begin() + (size_t)r * c.nodes);
+        }
+        std::vector<int> ts(c.noise_bw_it);
+        S.sh_ts.resize((size_t)c.noise_repeats * c.noise_bw_it);
+        std::iota(ts.begin(), ts.end(), 0);
+        for (int r = 0; r < c.noise_repeats; ++r) {
+            shuffle_positions(ts, gen);
+            std::copy(ts.begin(), ts.end(), S.sh_ts.begin() + (size_t)r * c.noise_bw_it);
+        }
+        S.d_noise.ensure(sizeof(double) * S.noise.size());
+        CK(cudaMemcpyAsync(S.d_noise.p, S.noise.data(), sizeof(double) * S.noise.size(), cudaMemcpyHostToDevice, S.st));
+        S.d_sh_nodes.ensure(sizeof(int) * S.sh_nodes.size());
+        CK(cudaMemcpyAsync(S.d_sh_nodes.p, S.sh_nodes.data(), sizeof(int) * S.sh_nodes.size(), cudaMemcpyHostToDevice, S.st));
+        S.d_sh_ts.ensure(sizeof(int) * S.sh_ts.size());
+        CK(cudaMemcpyAsync(S.d_sh_ts.p, S.sh_ts.data(), sizeof(int) * S.sh_ts.size(), cudaMemcpyHostToDevice, S.st));
+        CK(cudaStreamSynchronize(S.st));
+        S.noise_valid = true;
+        S.noise_f32_valid = false;
+        S.k_seed = c.sim_seed; S.k_time = c.time_steps; S.k_nodes = c.nodes; S.k_nts = c.noise_time_steps;
+        S.k_nnoise = md.n_noise; S.k_bwdt = c.bw_dt; S.k_dt = c.dt;
+    }
+    if (c.fp32 && !S.noise_f32_valid) {
+        std::vector<float> f(S.noise.begin(), S.noise.end());
+        S.d_noise_f32.ensure(sizeof(float) * f.size());
+        CK(cudaMemcpyAsync(S.d_noise_f32.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, S.st));
+        CK(cudaStreamSynchronize(S.st));
+        S.noise_f32_valid = true;
+    }
+}
+
+// ---------------------------------------------------------------- analytical FIC
+// Brent's method (Brent 1973; Numerical Recipes zbrent form) driven through
+// GSL's documented fsolver protocol: each iteration reports the bracket, the
+// caller stops when |hi-lo| < 1e-3 * min(|lo|,|hi|) (0 if the bracket holds 0),
+// at most 100 iterations, -1 on failure (rww_fic.cpp:62-102).
+template <class F>
+static double brent_root(F f, double x_lo, double x_hi) {
+    const double eps = 2.2204460492503131e-16;
+    double a = x_lo, b = x_hi, fa = f(a), fb = f(b);
+    if ((fa < 0.0 && fb < 0.0) || (fa > 0.0 && fb > 0.0)) return -1;
+    double c = b, fc = fb, d = b - a, e = b - a, root = 0.5 * (x_lo + x_hi);
+    for (int iter = 1; iter <= 100; ++iter) {
+        bool lin = false;
+        if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) { lin = true; c = a; fc = fa; d = b - a; e = b - a; }
+        if (std::fabs(fc) < std::fabs(fb)) { lin = true; a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+        const double tol = 0.5 * eps * std::fabs(b), m = 0.5 * (c - b);
+        double lo, hi;
+        if (fb == 0) {
+            root = b; lo = b; hi = b;
+        } else if (std::fabs(m) <= tol) {
+            root = b; lo = std::min(b, c); hi = std::max(b, c);
+        } else {
+            if (std::fabs(e) < tol || std::fabs(fa) <= std::fabs(fb)) {
+                d = m; e = m;
+            } else {
+                double p, q, r, s = fb / fa;
+                if (lin) { p = 2 * m * s; q = 1 - s; }
+                else {
+                    q = fa / fc; r = fb / fc;
+                    p = s * (2 * m * q * (q - r) - (b - a) * (r - 1));
+                    q = (q - 1) * (r - 1) * (s - 1);
+                }
+                if (p > 0) q = -q; else p = -p;
+                if (2 * p < std::min(3 * m * q - std::fabs(tol * q), std::fabs(e * q))) { e = d; d = p / q; }
+                else { d = m; e = m; }
+            }
+            a = b; fa = fb;
+            if (std::fabs(d) > tol) b += d; else b += (m > 0 ? +tol : -tol);
+            fb = f(b);
+            root = b;
+            double cc = c;
+            if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) cc = a;
+            if (b < cc) { lo = b; hi = cc; } else { lo = cc; hi = b; }
+        }
+        const double alo = std::fabs(lo), ahi = std::fabs(hi);
+        const double min_abs = ((lo > 0 && hi > 0) || (lo < 0 && hi < 0)) ? std::min(alo, ahi) : 0.0;
+        if (std::fabs(hi - lo) < 0.001 * min_abs) return root;
+    }
+    return -1;
+}
+
+// rww.cpp:73-146 + rww_fic.cpp:138-231; regional [n_r][N*n] host array, in/out.
+static void rww_analytical_fic(const Cfg &c, const cbnm_run_args *a, const double *gparams, double *regional,
+                               uint8_t *unstable, const RWWK &m) {
+    const int n = c.nodes;
+    const size_t stride = (size_t)c.n_sims * n;
+    const double I0_I = m.I_0 * m.w_I, I0_E = m.I_0 * m.w_E;
+    const double a_I = 615, b_I = 177, d_I = 0.087;  // rww.cpp:19-21
+    auto phi_I = [&](double II) { return ((a_I * II) - b_I) / (1 - std::exp(-1 * d_I * ((a_I * II) - b_I))); };
+    std::vector<double> w_IE(n);
+    for (int sim = 0; sim < c.n_sims; ++sim) {
+        const double *sc = a->sc + (size_t)a->sc_indices[sim] * n * n;
+        const double G = gparams[sim];
+        bool bad = false;
+        for (int j = 0; j < n && !bad; ++j) {
+            const double w_EI_j = regional[1 * stride + (size_t)sim * n + j];
+            const double w_EE_j = regional[0 * stride + (size_t)sim * n + j] * w_EI_j;
+            auto F = [&](double x) { return I0_I + w_EI_j * m.S_E_ss - m.w_II * m.gamma_I_s * m.tau_I_s * phi_I(x) - x; };
+            const double I_I = brent_root(F, 0.0, 2.0);
+            if (I_I == -1) { bad = true; break; }
+            const double r_I = phi_I(I_I);
+            const double S_I_ss = r_I * m.tau_I_s * m.gamma_I_s;
+            double dot = 0.0;
+            for (int k = 0; k < n; ++k) {
+                double kee = (sc[(size_t)k * n + j] * G) * w_EI_j;  // K_EE[j][k], SC transposed
+                if (k == j) kee = kee + w_EE_j;
+                dot += kee * m.S_E_ss;
+            }
+            const double w = (-1 / S_I_ss) * (m.I_E_ss - m.I_ext - I0_E - dot);
+            if (w < 0) { bad = true; break; }
+            w_IE[j] = w;
+        }
+        unstable[sim] = bad ? 1 : 0;
+        if (bad) std::fprintf(stderr, "In simulation #%d analytical FIC failed. Setting wIE to 1 in all nodes\n", sim);
+        for (int j = 0; j < n; ++j) regional[2 * stride + (size_t)sim * n + j] = bad ? 1.0 : w_IE[j];
+    }
+}
+
+// ---------------------------------------------------------------- helpers
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static void check_args(const cbnm_run_args *a) {
+    if (!a) throw Err(CBNM_ERR_ARG, "null arguments");
+    if (!a->sc || !a->sc_indices || !a->sc_dist || !a->global_params || !a->regional_params || !a->v_list)
+        throw Err(CBNM_ERR_ARG, "null input array");
+    if (a->n_scs <= 0) throw Err(CBNM_ERR_ARG, "n_scs must be positive");
+}
+
+static void fill_sizes(const Cfg &c, const ModelDesc &md, cbnm_sizes *sz) {
+    std::memset(sz, 0, sizeof(*sz));
+    sz->n_global_params = md.n_global; sz->n_regional_params = md.n_regional; sz->n_state_vars = md.n_state;
+    sz->n_global_out_bool = md.n_gout_bool; sz->n_global_out_int = md.n_gout_int;
+    sz->bold_len = c.bold_len; sz->n_pairs = c.n_pairs; sz->n_windows = c.n_windows;
+    sz->n_window_pairs = c.n_window_pairs; sz->states_len = c.states_len; sz->do_fc = c.do_fc; sz->do_fcd = c.do_fcd;
+    sz->modifies_params = md.modifies_params && c.do_fic;
+    sz->noise_repeats = c.noise_repeats; sz->noise_bw_it = c.noise_bw_it; sz->noise_size = c.noise_size;
+}
+
+// ---------------------------------------------------------------- run
+static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
+    const double t_begin = now_s();
+    check_args(a);
+    if (!o || !o->sim_bold) throw Err(CBNM_ERR_ARG, "null output arrays");
+    const ModelDesc *mdp = find_model(a->model_name);
+    if (!mdp) throw Err(CBNM_ERR_MODEL, std::string("Model ") + (a->model_name ? a->model_name : "(null)") + " not found");
+    const ModelDesc &md = *mdp;
+    if (a->use_cpu)
+        throw Err(CBNM_ERR_UNSUPPORTED, "use_cpu is not supported: this library runs the simulations on the GPU only");
+    Cfg c;
+    build_cfg(c, a, md);
+    if (c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this build");
+    if (c.do_fc && !o->sim_fc_trils) throw Err(CBNM_ERR_ARG, "do_fc is set but sim_fc_trils is null");
+    if (c.do_fcd && !o->sim_fcd_trils) throw Err(CBNM_ERR_ARG, "do_fcd is set but sim_fcd_trils is null");
+    if (c.ext_out && !o->sim_states) throw Err(CBNM_ERR_ARG, "ext_out is set but sim_states is null");
+    if (a->noise_out && (!o->noise || !o->shuffled_nodes || !o->shuffled_ts))
+        throw Err(CBNM_ERR_ARG, "noise_out is set but noise outputs are null");
+    for (int s = 0; s < c.n_sims && !device_io; ++s)
+        if (a->sc_indices[s] < 0 || a->sc_indices[s] >= a->n_scs) throw Err(CBNM_ERR_ARG, "SC index out of range");
+
+    Session &S = session();
+    cbnm_timing tm{};
+    const int N = c.n_sims, n = c.nodes;
+    const size_t nn = (size_t)n * n, gsize = (size_t)md.n_global * N, rsize = (size_t)md.n_regional * N * n;
+
+    // ---- init phase: noise (session cache), as init_gpu
+    const double t_init0 = now_s();
+    ensure_noise(S, c, md, a->force_reinit != 0);
+    const double init_time = now_s() - t_init0;
+
+    // ---- inputs
+    CK(cudaEventRecord(S.ev[0], S.st));
+    const double *d_sc = nullptr;
+    const int *d_sc_idx = nullptr;
+    const double *d_g = nullptr;
+    double *d_r = nullptr;
+    std::vector<double> h_g, h_r;
+    std::vector<uint8_t> h_gbools((size_t)md.n_gout_bool * N, 0);
+    std::vector<int32_t> h_sc_idx;
+    const double *h_sc = a->sc;
+    if (device_io) {
+        d_sc = a->sc; d_sc_idx = a->sc_indices; d_g = a->global_params; d_r = a->regional_params;
+        if (c.do_fic || c.fp32) {  // host copies needed for FIC / SC conversion
+            h_g.resize(gsize); h_r.resize(rsize);
+            CK(cudaMemcpyAsync(h_g.data(), a->global_params, sizeof(double) * gsize, cudaMemcpyDeviceToHost, S.st));
+            CK(cudaMemcpyAsync(h_r.data(), a->regional_params, sizeof(double) * rsize, cudaMemcpyDeviceToHost, S.st));
+            h_sc_idx.resize(N);
+            CK(cudaMemcpyAsync(h_sc_idx.data(), a->sc_indices, sizeof(int) * N, cudaMemcpyDeviceToHost, S.st));
+            CK(cudaStreamSynchronize(S.st));
+        }
+    } else {
+        S.d_sc.ensure(sizeof(double) * nn * a->n_scs);
+        CK(cudaMemcpyAsync(S.d_sc.p, a->sc, sizeof(double) * nn * a->n_scs, cudaMemcpyHostToDevice, S.st));
+        S.d_sc_idx.ensure(sizeof(int) * N);
+        CK(cudaMemcpyAsync(S.d_sc_idx.p, a->sc_indices, sizeof(int) * N, cudaMemcpyHostToDevice, S.st));
+        d_sc = S.d_sc.as<double>(); d_sc_idx = S.d_sc_idx.as<int>();
+        tm.h2d_bytes += sizeof(double) * nn * a->n_scs + sizeof(int) * N;
+        h_g.assign(a->global_params, a->global_params + gsize);
+        h_r.assign(a->regional_params, a->regional_params + rsize);
+    }
+    if (c.do_fic) {  // analytical FIC on the host (rww.cpp:73-146)
+        cbnm_run_args ha = *a;
+        std::vector<double> h_sc_copy;
+        if (device_io) {
+            h_sc_copy.resize(nn * a->n_scs);
+            CK(cudaMemcpy(h_sc_copy.data(), a->sc, sizeof(double) * nn * a->n_scs, cudaMemcpyDeviceToHost));
+            ha.sc = h_sc_copy.data();
+            ha.sc_indices = h_sc_idx.data();
+        }
+        rww_analytical_fic(c, &ha, h_g.data(), h_r.data(), h_gbools.data(), make_constants(MODEL_RWW, c.dt).rww);
+        if (device_io)
+            CK(cudaMemcpyAsync(a->regional_params, h_r.data(), sizeof(double) * rsize, cudaMemcpyHostToDevice, S.st));
+    }
+    if (!device_io) {
+        S.d_g.ensure(sizeof(double) * gsize);
+        S.d_r.ensure(sizeof(double) * rsize);
+        CK(cudaMemcpyAsync(S.d_g.p, h_g.data(), sizeof(double) * gsize, cudaMemcpyHostToDevice, S.st));
+        CK(cudaMemcpyAsync(S.d_r.p, h_r.data(), sizeof(double) * rsize, cudaMemcpyHostToDevice, S.st));
+        d_g = S.d_g.as<double>(); d_r = S.d_r.as<double>();
+        tm.h2d_bytes += sizeof(double) * (gsize + rsize);
+    }
+
+    // ---- delays (bnm.cpp:146-202: per-pair steps from the lower triangle, diagonal 1)
+    std::vector<double> h_v;
+    int has_delay = 0;
+    std::vector<int> h_delay, h_delay_idx(N, 0), h_max_delay(N, 0);
+    std::vector<long long> h_hist_off(N, 0);
+    long long hist_total = 0;
+    if (a->do_delay) {
+        h_v.resize(N);
+        std::vector<double> h_dist(nn);
+        if (device_io) {
+            CK(cudaMemcpy(h_v.data(), a->v_list, sizeof(double) * N, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(h_dist.data(), a->sc_dist, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+        } else {
+            h_v.assign(a->v_list, a->v_list + N);
+            h_dist.assign(a->sc_dist, a->sc_dist + nn);
+        }
+        std::map<double, int> table_of;
+        std::vector<int> table_max;
+        for (int s = 0; s < N; ++s) {
+            const double vel = h_v[s] * c.dt;
+            auto it = table_of.find(vel);
+            if (it == table_of.end()) {
+                const int t = (int)table_max.size();
+                table_of[vel] = t;
+                h_delay.resize((size_t)(t + 1) * nn, 0);
+                int *dl = h_delay.data() + (size_t)t * nn;
+                int mx = 0;
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j <= i; ++j) {
+                        if (i > j) {
+                            int dd = (int)rintf(h_dist[(size_t)i * n + j] / vel);
+                            dd = std::max(dd, 1);
+                            dl[(size_t)i * n + j] = dd;
+                            dl[(size_t)j * n + i] = dd;
+                            mx = std::max(mx, dd);
+                        } else {
+                            dl[(size_t)i * n + j] = 1;
+                        }
+                    }
+                table_max.push_back(mx);
+                it = table_of.find(vel);
+            }
+            h_delay_idx[s] = it->second;
+            h_max_delay[s] = table_max[it->second];
+        }
+        for (int s = 0; s < N; ++s) {
+            h_hist_off[s] = hist_total;
+            hist_total += (long long)h_max_delay[s] * n;
+        }
+        has_delay = *std::max_element(h_max_delay.begin(), h_max_delay.end()) > 0;
+    }
+    if (has_delay) {
+        S.d_delay.ensure(sizeof(int) * h_delay.size());
+        CK(cudaMemcpyAsync(S.d_delay.p, h_delay.data(), sizeof(int) * h_delay.size(), cudaMemcpyHostToDevice, S.st));
+        S.d_delay_idx.ensure(sizeof(int) * N);
+        CK(cudaMemcpyAsync(S.d_delay_idx.p, h_delay_idx.data(), sizeof(int) * N, cudaMemcpyHostToDevice, S.st));
+        S.d_max_delay.ensure(sizeof(int) * N);
+        CK(cudaMemcpyAsync(S.d_max_delay.p, h_max_delay.data(), sizeof(int) * N, cudaMemcpyHostToDevice, S.st));
+        S.d_hist_off.ensure(sizeof(long long) * N);
+        CK(cudaMemcpyAsync(S.d_hist_off.p, h_hist_off.data(), sizeof(long long) * N, cudaMemcpyHostToDevice, S.st));
+        if (c.fp32) S.d_hist_f32.ensure(sizeof(float) * hist_total);
+        else S.d_hist.ensure(sizeof(double) * hist_total);
+    }
+
+    // ---- outputs on the device
+    const size_t bold_n = (size_t)N * c.bold_len * n;
+    const size_t ext = c.states_ts ? (size_t)n * c.states_len : (size_t)n;
+    const size_t states_n = c.ext_out ? (size_t)md.n_state * N * ext : 0;
+    double *d_bold = device_io ? o->sim_bold : (double *)S.d_bold.ensure(sizeof(double) * bold_n);
+    double *d_states = device_io ? o->sim_states : (double *)S.d_states.ensure(sizeof(double) * std::max<size_t>(states_n, 1));
+    uint8_t *d_gbools = (uint8_t *)S.d_gbools.ensure(std::max<size_t>(1, (size_t)md.n_gout_bool * N));
+    int *d_gints = (int *)S.d_gints.ensure(sizeof(int) * std::max<size_t>(1, (size_t)md.n_gout_int * N));
+    if (md.n_gout_bool)
+        CK(cudaMemcpyAsync(d_gbools, h_gbools.data(), h_gbools.size(), cudaMemcpyHostToDevice, S.st));
+    if (md.n_gout_int) CK(cudaMemsetAsync(d_gints, 0, sizeof(int) * md.n_gout_int * N, S.st));
+    int *d_status = (int *)S.d_status.ensure(sizeof(int));
+    CK(cudaMemsetAsync(d_status, 0, sizeof(int), S.st));
+    CK(cudaEventRecord(S.ev[1], S.st));
+
+    // ---- integrate
+    IntegrateArgs ia;
+    std::memset(&ia, 0, sizeof(ia));
+    ia.nodes = n; ia.n_sims = N; ia.bw_it = c.bw_it; ia.inner_it = c.inner_it; ia.bold_tr_iters = c.bold_tr_iters;
+    ia.states_sampling_iters = c.states_sampling_iters; ia.n_states_samples_remove = c.n_states_samples_remove;
+    ia.noise_bw_it = c.noise_bw_it; ia.bold_len = c.bold_len; ia.states_len = c.states_len;
+    ia.ext_out = c.ext_out; ia.states_ts = c.states_ts;
+    ia.sc = d_sc; ia.sc_idx = d_sc_idx; ia.gparams = d_g; ia.rparams = d_r; ia.rparams_out = d_r;
+    ia.noise = S.d_noise.as<double>(); ia.noise_f32 = S.d_noise_f32.as<float>();
+    ia.sh_nodes = S.d_sh_nodes.as<int>(); ia.sh_ts = S.d_sh_ts.as<int>();
+    ia.has_delay = has_delay;
+    ia.delay = S.d_delay.as<int>(); ia.delay_idx = S.d_delay_idx.as<int>(); ia.max_delay = S.d_max_delay.as<int>();
+    ia.hist_off = S.d_hist_off.as<long long>(); ia.hist = S.d_hist.as<double>(); ia.hist_f32 = S.d_hist_f32.as<float>();
+    ia.bold = d_bold; ia.states = d_states; ia.gbools = d_gbools; ia.gints = d_gints;
+    ia.do_fic = c.do_fic; ia.max_fic_trials = c.max_fic_trials; ia.I_start = c.I_start; ia.I_end = c.I_end;
+    ia.I_dur = c.I_dur; ia.init_delta = c.init_delta;
+    ia.bw = g_bw; ia.bw.dt = c.bw_dt; ia.bw.dt_itau = ia.bw.dt * ia.bw.itau;  // core.cpp:291-292
+    ia.K = make_constants(md.id, c.dt);
+    ia.sim_begin = 0;
+    ia.n_regional = md.n_regional;
+    ia.status = d_status;
+    int launches = 0;
+    if (c.fp32) {
+        if (!fp32_supported(md.id, n, has_delay) || (c.do_fic && c.max_fic_trials > 0))
+            throw Err(CBNM_ERR_UNSUPPORTED, std::string("precision 'fp32' is not available for ") + md.name +
+                                                (has_delay ? " with delay" : "") +
+                                                (c.do_fic && c.max_fic_trials > 0 ? " with numerical FIC" : "") +
+                                                " at " + std::to_string(n) + " nodes; use precision 'fp64'");
+        // tiles of simulations that share one SC
+        const int TN = fp32_tile_sims();
+        std::vector<int> sc_of(N);
+        if (device_io) {
+            if (h_sc_idx.size() != (size_t)N) {
+                h_sc_idx.resize(N);
+                CK(cudaMemcpy(h_sc_idx.data(), a->sc_indices, sizeof(int) * N, cudaMemcpyDeviceToHost));
+            }
+            sc_of.assign(h_sc_idx.begin(), h_sc_idx.end());
+        } else {
+            sc_of.assign(a->sc_indices, a->sc_indices + N);
+        }
+        std::vector<int> order(N);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sc_of[x] < sc_of[y]; });
+        std::vector<int> tiles;
+        for (size_t i = 0; i < order.size();) {
+            const int sc = sc_of[order[i]];
+            tiles.push_back(sc);
+            int cnt = 0;
+            while (cnt < TN && i < order.size() && sc_of[order[i]] == sc) { tiles.push_back(order[i]); ++i; ++cnt; }
+            for (; cnt < TN; ++cnt) tiles.push_back(-1);
+        }
+        ia.n_tiles = (int)(tiles.size() / (TN + 1));
+        S.d_tiles.ensure(sizeof(int) * tiles.size());
+        CK(cudaMemcpyAsync(S.d_tiles.p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, S.st));
+        ia.tiles = S.d_tiles.as<int>();
+        // FP32 SC copy (converted once per run)
+        std::vector<float> f;
+        std::vector<double> tmp;
+        const double *src = h_sc;
+        if (device_io) {
+            tmp.resize(nn * a->n_scs);
+            CK(cudaMemcpy(tmp.data(), a->sc, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+            src = tmp.data();
+        }
+        f.assign(src, src + nn * a->n_scs);
+        S.d_sc_f32.ensure(sizeof(float) * f.size());
+        CK(cudaMemcpyAsync(S.d_sc_f32.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, S.st));
+        ia.sc_f32 = S.d_sc_f32.as<float>();
+        CK(cudaStreamSynchronize(S.st));
+        CK(cudaEventRecord(S.ev[1], S.st));
+        CK(launch_integrate_fp32(md.id, ia, S.st, &launches));
+    } else {
+        CK(launch_integrate_fp64(md.id, ia, S.st));
+        ++launches;
+    }
+    CK(cudaEventRecord(S.ev[2], S.st));
+
+    // ---- FC / FCD (bnm.cu:809-942), in chunks that bound the window-FC scratch
+    double *d_fc = nullptr, *d_fcd = nullptr;
+    if (c.do_fc) {
+        d_fc = device_io ? o->sim_fc_trils : (double *)S.d_fc.ensure(sizeof(double) * (size_t)N * c.n_pairs);
+        if (c.do_fcd) d_fcd = device_io ? o->sim_fcd_trils : (double *)S.d_fcd.ensure(sizeof(double) * std::max<size_t>(1, (size_t)N * c.n_window_pairs));
+        std::vector<int> pi, pj;
+        const int rh = n / 2;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < i; ++j) {
+                if (c.exc_inter && ((i < rh) ^ (j < rh))) continue;
+                pi.push_back(i);
+                pj.push_back(j);
+            }
+        S.d_pairs_i.ensure(sizeof(int) * pi.size());
+        S.d_pairs_j.ensure(sizeof(int) * pj.size());
+        CK(cudaMemcpyAsync(S.d_pairs_i.p, pi.data(), sizeof(int) * pi.size(), cudaMemcpyHostToDevice, S.st));
+        CK(cudaMemcpyAsync(S.d_pairs_j.p, pj.data(), sizeof(int) * pj.size(), cudaMemcpyHostToDevice, S.st));
+        int max_T = c.corr_len;
+        if (c.do_fcd) {
+            S.d_wstart.ensure(sizeof(int) * c.n_windows);
+            S.d_wend.ensure(sizeof(int) * c.n_windows);
+            CK(cudaMemcpyAsync(S.d_wstart.p, c.w_start.data(), sizeof(int) * c.n_windows, cudaMemcpyHostToDevice, S.st));
+            CK(cudaMemcpyAsync(S.d_wend.p, c.w_end.data(), sizeof(int) * c.n_windows, cudaMemcpyHostToDevice, S.st));
+            for (int w = 0; w < c.n_windows; ++w) max_T = std::max(max_T, c.w_end[w] - c.w_start[w] + 1);
+        }
+        const size_t per_sim = sizeof(double) * (size_t)std::max(1, c.n_windows) * c.n_pairs;
+        const size_t budget = (size_t)1 << 30;
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(N, budget / per_sim));
+        if (c.do_fcd) S.d_wfc.ensure(per_sim * chunk);
+        FcArgs fa;
+        std::memset(&fa, 0, sizeof(fa));
+        fa.nodes = n; fa.bold_len = c.bold_len; fa.n_vols_remove = c.n_vols_remove; fa.n_pairs = c.n_pairs;
+        fa.n_windows = c.do_fcd ? c.n_windows : 0; fa.n_window_pairs = c.n_window_pairs; fa.max_T = max_T;
+        fa.w_start = S.d_wstart.as<int>(); fa.w_end = S.d_wend.as<int>();
+        fa.pair_i = S.d_pairs_i.as<int>(); fa.pair_j = S.d_pairs_j.as<int>();
+        fa.bold = d_bold; fa.fc = d_fc; fa.fcd = d_fcd; fa.wfc = S.d_wfc.as<double>();
+        for (int s0 = 0; s0 < N; s0 += chunk) {
+            fa.sim_begin = s0;
+            fa.sim_count = std::min(chunk, N - s0);
+            CK(launch_fc(fa, S.st, &launches));
+        }
+    }
+    CK(cudaEventRecord(S.ev[3], S.st));
+
+    // ---- outputs back to the host (bnm.cu:951-971) and parameter write-back
+    if (!device_io) {
+        CK(cudaMemcpyAsync(o->sim_bold, d_bold, sizeof(double) * bold_n, cudaMemcpyDeviceToHost, S.st));
+        tm.d2h_bytes += sizeof(double) * bold_n;
+        if (c.do_fc) {
+            CK(cudaMemcpyAsync(o->sim_fc_trils, d_fc, sizeof(double) * (size_t)N * c.n_pairs, cudaMemcpyDeviceToHost, S.st));
+            tm.d2h_bytes += sizeof(double) * (size_t)N * c.n_pairs;
+            if (c.do_fcd) {
+                CK(cudaMemcpyAsync(o->sim_fcd_trils, d_fcd, sizeof(double) * (size_t)N * c.n_window_pairs, cudaMemcpyDeviceToHost, S.st));
+                tm.d2h_bytes += sizeof(double) * (size_t)N * c.n_window_pairs;
+            }
+        }
+        if (c.ext_out) {
+            CK(cudaMemcpyAsync(o->sim_states, d_states, sizeof(double) * states_n, cudaMemcpyDeviceToHost, S.st));
+            tm.d2h_bytes += sizeof(double) * states_n;
+        }
+        if (md.modifies_params && c.do_fic) {  // core.cpp:437-450
+            CK(cudaMemcpyAsync(a->regional_params, d_r, sizeof(double) * rsize, cudaMemcpyDeviceToHost, S.st));
+            tm.d2h_bytes += sizeof(double) * rsize;
+        }
+    }
+    if (md.n_gout_bool && o->global_bools) {
+        CK(cudaMemcpyAsync(o->global_bools, d_gbools, (size_t)md.n_gout_bool * N,
+                           device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, S.st));
+    }
+    if (md.n_gout_int && o->global_ints) {
+        CK(cudaMemcpyAsync(o->global_ints, d_gints, sizeof(int) * md.n_gout_int * N,
+                           device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, S.st));
+    }
+    int h_status = 0;
+    CK(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, S.st));
+    CK(cudaEventRecord(S.ev[4], S.st));
+    CK(cudaStreamSynchronize(S.st));
+    if (h_status != 0)
+        throw Err(CBNM_ERR_TIMEOUT, "a device-side wait in the integrator gave up (status " + std::to_string(h_status) + ")");
+    if (a->noise_out) {  // core.cpp:429-435
+        if (device_io) {
+            CK(cudaMemcpy(o->noise, S.d_noise.p, sizeof(double) * S.noise.size(), cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(o->shuffled_nodes, S.d_sh_nodes.p, sizeof(int) * S.sh_nodes.size(), cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(o->shuffled_ts, S.d_sh_ts.p, sizeof(int) * S.sh_ts.size(), cudaMemcpyDeviceToDevice));
+        } else {
+            std::memcpy(o->noise, S.noise.data(), sizeof(double) * S.noise.size());
+            std::memcpy(o->shuffled_nodes, S.sh_nodes.data(), sizeof(int) * S.sh_nodes.size());
+            std::memcpy(o->shuffled_ts, S.sh_ts.data(), sizeof(int) * S.sh_ts.size());
+        }
+    }
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[1])); tm.h2d_ms = ms;
+    CK(cudaEventElapsedTime(&ms, S.ev[1], S.ev[2])); tm.integrate_ms = ms;
+    CK(cudaEventElapsedTime(&ms, S.ev[2], S.ev[3])); tm.fc_ms = ms;
+    CK(cudaEventElapsedTime(&ms, S.ev[3], S.ev[4])); tm.d2h_ms = ms;
+    CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[4])); tm.total_ms = ms;
+    tm.kernel_launches = launches;
+    S.timing = tm;
+    o->init_time = init_time;
+    o->run_time = now_s() - t_begin - init_time;
+}
+
+// ---------------------------------------------------------------- GOF
+static void gof_impl(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc, const double *sim_fcd,
+                     int n_wp, const double *emp_fcd, int n_emp_fcd, double *fc_corr, double *fc_diff,
+                     double *fc_normec, double *fcd_ks) {
+    if (n_sims <= 0) return;
+    Session &S = session();
+    GofArgs g;
+    std::memset(&g, 0, sizeof(g));
+    g.n_sims = n_sims; g.n_pairs = n_pairs; g.n_wp = n_wp; g.n_emp_fcd = n_emp_fcd;
+    const bool want_fc = sim_fc && emp_fc && n_pairs > 0 && (fc_corr || fc_diff || fc_normec);
+    const bool want_ks = sim_fcd && emp_fcd && n_wp > 0 && n_emp_fcd > 0 && fcd_ks;
+    double *d_out = (double *)S.g_out.ensure(sizeof(double) * 4 * n_sims);
+    if (want_fc) {
+        double m = 0;
+        for (int p = 0; p < n_pairs; ++p) m += emp_fc[p];
+        m /= n_pairs;
+        double q = 0;
+        for (int p = 0; p < n_pairs; ++p) q += (emp_fc[p] - m) * (emp_fc[p] - m);
+        g.emp_fc_mean = m; g.emp_fc_ssd = std::sqrt(q);
+        S.g_simfc.ensure(sizeof(double) * (size_t)n_sims * n_pairs);
+        S.g_empfc.ensure(sizeof(double) * n_pairs);
+        CK(cudaMemcpyAsync(S.g_simfc.p, sim_fc, sizeof(double) * (size_t)n_sims * n_pairs, cudaMemcpyHostToDevice, S.st));
+        CK(cudaMemcpyAsync(S.g_empfc.p, emp_fc, sizeof(double) * n_pairs, cudaMemcpyHostToDevice, S.st));
+        g.sim_fc = S.g_simfc.as<double>(); g.emp_fc = S.g_empfc.as<double>();
+        if (fc_corr) g.fc_corr = d_out;
+        if (fc_diff) g.fc_diff = d_out + n_sims;
+        if (fc_normec) g.fc_normec = d_out + 2 * n_sims;
+    }
+    std::vector<double> emp_sorted;
+    if (want_ks) {
+        if (sizeof(double) * (size_t)n_wp > gof_ks_smem_limit())
+            throw Err(CBNM_ERR_UNSUPPORTED, "FCD too long for the KS kernel");
+        emp_sorted.assign(emp_fcd, emp_fcd + n_emp_fcd);
+        std::sort(emp_sorted.begin(), emp_sorted.end());
+        S.g_simfcd.ensure(sizeof(double) * (size_t)n_sims * n_wp);
+        S.g_empfcd.ensure(sizeof(double) * n_emp_fcd);
+        CK(cudaMemcpyAsync(S.g_simfcd.p, sim_fcd, sizeof(double) * (size_t)n_sims * n_wp, cudaMemcpyHostToDevice, S.st));
+        CK(cudaMemcpyAsync(S.g_empfcd.p, emp_sorted.data(), sizeof(double) * n_emp_fcd, cudaMemcpyHostToDevice, S.st));
+        g.sim_fcd = S.g_simfcd.as<double>(); g.emp_fcd_sorted = S.g_empfcd.as<double>();
+        g.fcd_ks = d_out + 3 * n_sims;
+    }
+    int launches = 0;
+    CK(launch_gof(g, S.st, &launches));
+    std::vector<double> h((size_t)4 * n_sims);
+    CK(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, S.st));
+    CK(cudaStreamSynchronize(S.st));
+    if (want_fc && fc_corr) std::memcpy(fc_corr, h.data(), sizeof(double) * n_sims);
+    if (want_fc && fc_diff) std::memcpy(fc_diff, h.data() + n_sims, sizeof(double) * n_sims);
+    if (want_fc && fc_normec) std::memcpy(fc_normec, h.data() + 2 * n_sims, sizeof(double) * n_sims);
+    if (want_ks) {
+        std::memcpy(fcd_ks, h.data() + 3 * n_sims, sizeof(double) * n_sims);
+        for (int s = 0; s < n_sims; ++s)  // a NaN in a row makes the statistic NaN
+            for (int p = 0; p < n_wp; ++p)
+                if (std::isnan(sim_fcd[(size_t)s * n_wp + p])) { fcd_ks[s] = NAN; break; }
+    }
+}
+
+}  // namespace cbnm
+
+// ---------------------------------------------------------------- C ABI
+using namespace cbnm;
+
+template <class F>
+static int guarded(F f) {
+    try {
+        f();
+        g_err.clear();
+        return CBNM_OK;
+    } catch (const Err &e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return CBNM_ERR_CONFIG;
+    }
+}
+
+extern "C" {
+
+int cbnm_init(void) {
+    g_bw = bw_defaults(0.001);
+    return CBNM_OK;
+}
+
+int cbnm_set_const(const char *key, double value) {
+    if (!key) { g_err = "null key"; return CBNM_ERR_ARG; }
+    const std::string k = key;
+    if (k == "k1") g_bw.k1 = value;
+    else if (k == "k2") g_bw.k2 = value;
+    else if (k == "k3") g_bw.k3 = value;
+    else if (k == "V_0") g_bw.V_0 = value;
+    g_bw.V_0_k1 = g_bw.V_0 * g_bw.k1;
+    g_bw.V_0_k2 = g_bw.V_0 * g_bw.k2;
+    g_bw.V_0_k3 = g_bw.V_0 * g_bw.k3;
+    return CBNM_OK;
+}
+
+int cbnm_query_sizes(const cbnm_run_args *a, cbnm_sizes *sz) {
+    return guarded([&] {
+        if (!a || !sz) throw Err(CBNM_ERR_ARG, "null argument");
+        const ModelDesc *md = find_model(a->model_name);
+        if (!md) throw Err(CBNM_ERR_MODEL, std::string("Model ") + (a->model_name ? a->model_name : "(null)") + " not found");
+        Cfg c;
+        build_cfg(c, a, *md);
+        fill_sizes(c, *md, sz);
+    });
+}
+
+int cbnm_run_simulations(const cbnm_run_args *a, cbnm_outputs *o) {
+    return guarded([&] { run_impl(a, o, false); });
+}
+
+int cbnm_run_simulations_device(const cbnm_run_args *a, cbnm_outputs *o) {
+    return guarded([&] { run_impl(a, o, true); });
+}
+
+int cbnm_last_timing(cbnm_timing *t) {
+    if (!t) return CBNM_ERR_ARG;
+    if (g_sess) *t = g_sess->timing;
+    else std::memset(t, 0, sizeof(*t));
+    return CBNM_OK;
+}
+
+int cbnm_reset(void) {
+    return guarded([&] { release_session(); });
+}
+
+const char *cbnm_last_error(void) { return g_err.c_str(); }
+
+int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc, const double *sim_fcd,
+             int n_window_pairs, const double *emp_fcd, int n_emp_fcd, double *fc_corr, double *fc_diff,
+             double *fc_normec, double *fcd_ks) {
+    return guarded([&] {
+        gof_impl(sim_fc, n_sims, n_pairs, emp_fc, sim_fcd, n_window_pairs, emp_fcd, n_emp_fcd, fc_corr, fc_diff,
+                 fc_normec, fcd_ks);
+    });
+}
+
+}  // extern "C"

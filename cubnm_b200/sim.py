@@ -1,0 +1,413 @@
+"""SimGroup classes with the reference's run / score interface.
+
+Restates the parts of src/cubnm/sim/base.py that sit on the simulation path
+(``SimGroup.__init__`` settings, ``run`` base.py:673-766, ``_process_out``
+:768-818, ``get_noise`` :843-895, ``score`` :1084-1207,
+``MultiSimGroupMixin`` :1303-1438) and the per-model parameter surface of
+src/cubnm/sim/{rww,wc,jr,kuramoto,rwwex}.py.  Simulations run through
+``cubnm_b200.core.run_simulations``; the goodness-of-fit terms through the
+library's GPU kernels.  Plotting / saving helpers are not part of this path.
+"""
+import copy
+from decimal import Decimal
+
+import numpy as np
+import pandas as pd
+
+from . import core, utils
+
+WORST_SCORES = {"+fc_corr": -1.0, "-fc_diff": -2.0, "-fc_normec": -1.0, "-fcd_ks": -1.0}
+
+
+class SimGroup:
+    model_name = None
+    global_param_names = []
+    regional_param_names = []
+    state_names = []
+    sel_state_var = None
+    n_noise = 1
+    default_params = {}
+
+    def __init__(self, duration, TR, sc, sc_dist=None, out_dir=None, dt="0.1", bw_dt="1.0", states_ts=False,
+                 states_sampling=None, noise_out=False, do_fc=True, do_fcd=True, window_size=30, window_step=5,
+                 sim_seed=0, exc_interhemispheric=False, force_cpu=False, force_gpu=False,
+                 gof_terms=("+fc_corr", "-fcd_ks"), bw_params="friston2003", bold_remove_s=30,
+                 fcd_drop_edges=True, noise_segment_length=30, sim_verbose=False, progress_interval=500,
+                 precision="fp64"):
+        if force_cpu:
+            raise ValueError("force_cpu is not supported: cubnm_b200 runs the simulations on the GPU")
+        self.sc = np.asarray(sc, dtype=float)
+        self.nodes = self.sc.shape[-1]
+        self.duration = duration
+        self.duration_msec = int(Decimal(str(duration)) * 1000)
+        self.TR = TR
+        self.TR_msec = int(TR * 1000)
+        self.states_sampling = TR if states_sampling is None else states_sampling
+        self.states_sampling_msec = int(self.states_sampling * 1000)
+        self._dt = Decimal(dt)
+        self._bw_dt = Decimal(bw_dt)
+        assert self._bw_dt >= self._dt and self._bw_dt % self._dt == 0, "bw_dt must be a multiple of dt"
+        assert Decimal(self.duration_msec) % self._bw_dt == 0, "duration must be a multiple of bw_dt"
+        self.states_ts = states_ts
+        self.noise_out = noise_out
+        self.gof_terms = list(gof_terms)
+        self.do_fc = do_fc
+        self.do_fcd = do_fcd and do_fc
+        self.window_size = window_size
+        self.window_step = window_step
+        self.window_size_TRs = int(np.round(window_size / (TR * 2))) * 2  # base.py:468-476
+        self.window_step_TRs = int(np.round(window_step / TR))
+        self.sim_seed = sim_seed
+        self.exc_interhemispheric = exc_interhemispheric
+        self.bold_remove_s = bold_remove_s
+        self.fcd_drop_edges = fcd_drop_edges
+        self.noise_segment_length = duration if noise_segment_length is None else noise_segment_length
+        self.sim_verbose = sim_verbose
+        self.progress_interval = progress_interval
+        self.precision = precision
+        if sc_dist is None:
+            self.sc_dist = np.zeros((self.nodes, self.nodes))
+            self.do_delay = False
+        else:
+            self.sc_dist = np.asarray(sc_dist, dtype=float)
+            self.do_delay = True
+        self.bw_params = bw_params
+        p = utils.get_bw_params(bw_params) if isinstance(bw_params, str) else bw_params
+        for k in ("k1", "k2", "k3"):
+            core.set_const(k, p[k])
+        self.param_lists = {k: None for k in self.global_param_names + self.regional_param_names + ["v"]}
+        self.last_N = 0
+        self.last_config = self.get_config()
+        self.it = 0
+        self._N = 0
+
+    # -- properties mirrored from base.py
+    @property
+    def N(self):
+        return self._N
+
+    @N.setter
+    def N(self, N):
+        self._N = N
+        if not self.do_delay:
+            self.param_lists["v"] = np.zeros(N, dtype=float)
+
+    @property
+    def dt(self):
+        return self._dt
+
+    @property
+    def bw_dt(self):
+        return self._bw_dt
+
+    @property
+    def bw_it(self):
+        return int(self.duration_msec / self.bw_dt)
+
+    @property
+    def inner_it(self):
+        return int(self.bw_dt / self.dt)
+
+    @property
+    def n_states_samples_remove(self):
+        return int(self.bold_remove_s / self.states_sampling)
+
+    def get_config(self):
+        return {
+            "duration": self.duration, "TR": self.TR, "nodes": self.nodes, "states_ts": self.states_ts,
+            "states_sampling": self.states_sampling, "do_fc": self.do_fc, "do_fcd": self.do_fcd,
+            "window_size_TRs": self.window_size_TRs, "window_step_TRs": self.window_step_TRs,
+            "sim_seed": self.sim_seed, "exc_interhemispheric": self.exc_interhemispheric,
+            "bold_remove_s": self.bold_remove_s, "fcd_drop_edges": self.fcd_drop_edges,
+            "noise_segment_length": self.noise_segment_length, "precision": self.precision,
+        }
+
+    @property
+    def _model_config(self):  # base.py:635-657
+        return {
+            "do_fc": str(int(self.do_fc)),
+            "do_fcd": str(int(self.do_fcd)),
+            "bold_remove_s": str(self.bold_remove_s),
+            "exc_interhemispheric": str(int(self.exc_interhemispheric)),
+            "window_size": str(self.window_size_TRs),
+            "window_step": str(self.window_step_TRs),
+            "drop_edges": str(int(self.fcd_drop_edges)),
+            "noise_time_steps": str(int(self.noise_segment_length * 1000)),
+            "verbose": str(int(self.sim_verbose)),
+            "progress_interval": str(int(self.progress_interval)),
+            "precision": self.precision,
+        }
+
+    def _set_default_params(self, missing=True):  # base.py:532-575
+        defaults = copy.copy(self.default_params)
+        if self.do_delay and "v" not in defaults:
+            defaults["v"] = 0.5
+        for param, v in defaults.items():
+            cur = self.param_lists.get(param)
+            if (not missing) or cur is None or np.asarray(cur).shape[0] != self.N:
+                if v is None:
+                    raise ValueError(f"Parameter {param} does not have a default value and must be set")
+                if param in self.global_param_names or param == "v":
+                    self.param_lists[param] = np.repeat(v, self.N).astype(float)
+                else:
+                    if param == "wIE" and getattr(self, "do_fic", False):
+                        continue
+                    self.param_lists[param] = np.full((self.N, self.nodes), v, dtype=float)
+
+    def _run_args(self, force_reinit):
+        self._global_params = np.vstack(
+            [np.ascontiguousarray(self.param_lists[p], dtype=float)[None, :] for p in self.global_param_names])
+        self._regional_params = np.vstack(
+            [np.ascontiguousarray(np.asarray(self.param_lists[p], dtype=float).flatten()) for p in self.regional_param_names])
+        if self.sc.ndim == 2 or self.sc.shape[0] == 1:
+            sc = np.ascontiguousarray(self.sc.reshape(-1))[None, :]
+            sc_indices = np.zeros(self.N, dtype=np.intc)
+        else:
+            sc = np.ascontiguousarray(self.sc.reshape(self.sc.shape[0], -1))
+            sc_indices = np.ascontiguousarray(np.asarray(self.sc_indices).astype(np.intc))
+        return (self.model_name, sc, sc_indices, np.ascontiguousarray(self.sc_dist.flatten()), self._global_params,
+                self._regional_params, np.ascontiguousarray(self.param_lists["v"], dtype=float), self._model_config,
+                True, self.states_ts, self.noise_out, self.do_delay, force_reinit, False, self.N, self.nodes,
+                self.duration_msec, self.TR_msec, self.states_sampling_msec, self.sim_seed, float(self.dt),
+                float(self.bw_dt))
+
+    def run(self, force_reinit=False):  # base.py:673-766
+        cfg = self.get_config()
+        force_reinit = force_reinit or (self.N != self.last_N) or (cfg != self.last_config)
+        out = core.run_simulations(*self._run_args(force_reinit))
+        self.last_N = self.N
+        self.last_config = cfg
+        self.it += 1
+        self._process_out(out)
+
+    def _process_out(self, out):  # base.py:768-818
+        self.__dict__.update(out)
+        self.sim_bold = self.sim_bold.reshape(self.N, -1, self.nodes)
+        self.sim_states = {}
+        for i, name in enumerate(self.state_names):
+            self.sim_states[name] = self._sim_states[i, :, :]
+            if self.states_ts:
+                self.sim_states[name] = self.sim_states[name].reshape(self.N, -1, self.nodes)
+        if self.do_fc:
+            self.sim_fc_trils = self.sim_fc_trils.reshape(self.N, -1)
+            if self.do_fcd:
+                self.sim_fcd_trils = self.sim_fcd_trils.reshape(self.N, -1)
+
+    def get_noise(self):  # base.py:843-895
+        if not self.noise_out:
+            raise ValueError("Noise was not saved in the simulation. Set `noise_out` to true and redo the simulation.")
+        seg_outer = int(int(self.noise_segment_length * 1000) / self.bw_dt)
+        seg = self._noise.reshape(seg_outer, self.inner_it, self.nodes, -1)
+        parts = [seg[self._shuffled_ts[r]][:, :, self._shuffled_nodes[r]] for r in range(self._shuffled_nodes.shape[0])]
+        return np.concatenate(parts, axis=0)[: self.bw_it].transpose(3, 2, 0, 1)
+
+    def score(self, emp_fc_tril=None, emp_fcd_tril=None, emp_bold=None, force_cpu=False, usable_mem=None):
+        """Goodness-of-fit terms per simulation (base.py:1084-1207), computed on the GPU."""
+        if emp_bold is not None:
+            if self.do_fc:
+                emp_fc_tril = utils.calculate_fc(emp_bold, self.exc_interhemispheric, return_tril=True)
+            if self.do_fcd:
+                emp_fcd_tril = utils.calculate_fcd(emp_bold, self.window_size_TRs, self.window_step_TRs,
+                                                   drop_edges=self.fcd_drop_edges,
+                                                   exc_interhemispheric=self.exc_interhemispheric,
+                                                   return_tril=True, return_dfc=False)
+        columns = []
+        if self.do_fc and emp_fc_tril is not None:
+            columns += [c for c in ["+fc_corr", "-fc_diff", "-fc_normec"] if c in self.gof_terms]
+            assert emp_fc_tril.size == self.sim_fc_trils.shape[1], \
+                "Empirical FC lower triangle size does not match the simulated FC size"
+        if self.do_fcd and emp_fcd_tril is not None:
+            columns += [c for c in ["-fcd_ks"] if c in self.gof_terms]
+        columns += ["+gof"]
+        scores = pd.DataFrame(index=range(self.N), columns=columns, dtype=float)
+        want = [c[1:] for c in columns if c != "+gof"]
+        res = utils.gof(
+            sim_fc_trils=self.sim_fc_trils if self.do_fc and emp_fc_tril is not None else None,
+            emp_fc_tril=emp_fc_tril,
+            sim_fcd_trils=self.sim_fcd_trils if self.do_fcd and emp_fcd_tril is not None else None,
+            emp_fcd_tril=emp_fcd_tril, terms=want)
+        sign = {"fc_corr": 1.0, "fc_diff": -1.0, "fc_normec": -1.0, "fcd_ks": -1.0}
+        for c in columns:
+            if c != "+gof":
+                scores.loc[:, c] = sign[c[1:]] * res[c[1:]]
+                scores.loc[:, c] = scores.loc[:, c].fillna(WORST_SCORES.get(c, np.nan))
+        scores.loc[:, "+gof"] = scores.loc[:, [c for c in self.gof_terms if c in scores.columns]].sum(axis=1)
+        return scores
+
+
+class rWWSimGroup(SimGroup):
+    """Reduced Wong-Wang E-I model (src/cubnm/sim/rww.py)."""
+    model_name = "rWW"
+    global_param_names = ["G"]
+    regional_param_names = ["w_p", "J_N", "wIE", "sigma"]
+    state_names = ["I_E", "I_I", "r_E", "r_I", "S_E", "S_I"]
+    sel_state_var = "r_E"
+    n_noise = 2
+    default_params = {"G": None, "w_p": 1.4, "J_N": 0.15, "wIE": 1.0, "sigma": 0.01}
+
+    def __init__(self, *args, do_fic=True, max_fic_trials=0, I_SAMPLING_START=1000, I_SAMPLING_END=10000,
+                 init_delta=0.02, fic_penalty_scale=0.5, **kwargs):
+        self.do_fic = do_fic
+        self.max_fic_trials = max_fic_trials
+        self.I_SAMPLING_START = I_SAMPLING_START
+        self.I_SAMPLING_END = I_SAMPLING_END
+        self.init_delta = init_delta
+        self.fic_penalty_scale = fic_penalty_scale
+        super().__init__(*args, **kwargs)
+
+    @SimGroup.N.setter
+    def N(self, N):
+        SimGroup.N.fset(self, N)
+        if self.do_fic:
+            self.param_lists["wIE"] = np.zeros((N, self.nodes), dtype=float)
+
+    @property
+    def _model_config(self):
+        cfg = super()._model_config
+        cfg.update({"do_fic": str(int(self.do_fic)), "max_fic_trials": str(self.max_fic_trials),
+                    "I_SAMPLING_START": str(self.I_SAMPLING_START), "I_SAMPLING_END": str(self.I_SAMPLING_END),
+                    "init_delta": str(self.init_delta), "fic_penalty_scale": str(self.fic_penalty_scale)})
+        return cfg
+
+    def _process_out(self, out):  # rww.py:170-178
+        super()._process_out(out)
+        if self.do_fic:
+            self.fic_unstable = self._global_bools[0]
+            self.fic_failed = self._global_bools[1]
+            self.fic_ntrials = self._global_ints[0]
+            self.param_lists["wIE"] = self._regional_params[2].reshape(self.N, -1)
+
+    def score(self, emp_fc_tril=None, emp_fcd_tril=None, emp_bold=None, **kwargs):  # rww.py:180-234
+        scores = super().score(emp_fc_tril, emp_fcd_tril, emp_bold, **kwargs)
+        if self.do_fic and self.fic_penalty_scale > 0:
+            mean_r_E = self.sim_states["r_E"]
+            if self.states_ts:
+                mean_r_E = mean_r_E[:, self.n_states_samples_remove:].mean(axis=1)
+            for idx in range(self.N):
+                diff = np.abs(mean_r_E[idx, :] - 3)
+                if (diff > 1).sum() > 0:
+                    diff[diff <= 1] = np.nan
+                    scores.loc[idx, "-fic_penalty"] = (
+                        -np.nansum(1 - np.exp(-0.05 * (diff - 1))) * self.fic_penalty_scale / self.nodes)
+                else:
+                    scores.loc[idx, "-fic_penalty"] = 0
+        return scores
+
+
+class WCSimGroup(SimGroup):
+    """Wilson-Cowan E-I model (src/cubnm/sim/wc.py)."""
+    model_name = "WC"
+    global_param_names = ["G"]
+    regional_param_names = ["c_EE", "c_IE", "c_EI", "c_II", "P_E", "P_I", "sigma_E", "sigma_I"]
+    state_names = ["E", "I"]
+    sel_state_var = "E"
+    n_noise = 2
+    default_params = {"G": None, "c_EE": 16, "c_IE": 12, "c_EI": 15, "c_II": 3, "P_E": 0.5, "P_I": 0.0,
+                      "sigma_E": 5e-05, "sigma_I": 5e-05}
+
+
+class JRSimGroup(SimGroup):
+    """Jansen-Rit model (src/cubnm/sim/jr.py)."""
+    model_name = "JR"
+    global_param_names = ["G"]
+    regional_param_names = ["J", "a_1", "a_2", "a_3", "a_4", "sigma"]
+    state_names = ["y0", "y1", "y2", "y3", "y4", "y5", "y1_y2", "s_y1_y2"]
+    sel_state_var = "y1_y2"
+    n_noise = 1
+    default_params = {"G": None, "J": 135.0, "a_1": 1.0, "a_2": 0.8, "a_3": 0.25, "a_4": 0.25, "sigma": 0.0001}
+
+
+class KuramotoSimGroup(SimGroup):
+    """Kuramoto oscillators (src/cubnm/sim/kuramoto.py)."""
+    model_name = "Kuramoto"
+    global_param_names = ["G"]
+    regional_param_names = ["init_theta", "omega", "sigma"]
+    state_names = ["theta"]
+    sel_state_var = "theta"
+    n_noise = 1
+    default_params = {"G": None, "init_theta": None, "omega": np.pi, "sigma": 0.17}
+
+    def __init__(self, *args, random_init_theta=True, **kwargs):
+        self.random_init_theta = random_init_theta
+        super().__init__(*args, **kwargs)
+
+    @SimGroup.N.setter
+    def N(self, N):
+        SimGroup.N.fset(self, N)
+        if self.random_init_theta:  # kuramoto.py:120-133
+            rng = np.random.default_rng(self.sim_seed)
+            self.param_lists["init_theta"] = np.tile(rng.uniform(0, 2 * np.pi, self.nodes), (N, 1))
+        else:
+            self.param_lists["init_theta"] = np.zeros((N, self.nodes), dtype=float)
+
+    @property
+    def _model_config(self):
+        cfg = super()._model_config
+        cfg["random_init_theta"] = str(int(self.random_init_theta))
+        return cfg
+
+
+class rWWExSimGroup(SimGroup):
+    """Excitatory-only reduced Wong-Wang model (src/cubnm/sim/rwwex.py)."""
+    model_name = "rWWEx"
+    global_param_names = ["G"]
+    regional_param_names = ["w", "I0", "sigma"]
+    state_names = ["x", "r", "S"]
+    sel_state_var = "r"
+    n_noise = 1
+    default_params = {"G": None, "w": 0.9, "I0": 0.3, "sigma": 0.001}
+
+
+class MultiSimGroupMixin:
+    """Runs several SimGroups as one launch (base.py:1303-1438)."""
+
+    def __init__(self, sim_groups):
+        self.children = sim_groups
+        self.__dict__.update(copy.deepcopy({k: v for k, v in sim_groups[0].__dict__.items() if k != "children"}))
+
+    @property
+    def N(self):
+        return sum(child.N for child in self.children)
+
+    def run(self, **kwargs):
+        scs, idx = [], []
+        for child in self.children:
+            cs = child.sc if child.sc.ndim == 3 else child.sc[None]
+            ci = np.zeros(child.N, dtype=int) if cs.shape[0] == 1 else np.asarray(child.sc_indices)
+            remap = {}
+            for k, m in enumerate(cs):
+                hit = [i for i, s in enumerate(scs) if np.allclose(s, m)]
+                if hit:
+                    remap[k] = hit[0]
+                else:
+                    scs.append(m)
+                    remap[k] = len(scs) - 1
+            idx.append(np.array([remap[k] for k in ci], dtype=int))
+        self.sc = np.stack(scs) if len(scs) > 1 else scs[0]
+        self.sc_indices = np.concatenate(idx)
+        for p in self.param_lists:
+            self.param_lists[p] = np.concatenate([np.asarray(c.param_lists[p]) for c in self.children])
+        self._N = self.N
+        SimGroup.run(self, **kwargs)
+
+    def _process_out(self, out):
+        start = 0
+        for child in self.children:
+            end = start + child.N
+            child._regional_params = self._regional_params[:, start * child.nodes:end * child.nodes]
+            child._global_params = self._global_params[:, start:end]
+            oc = {}
+            for k, v in out.items():
+                if k in ("init_time", "run_time", "_noise", "_shuffled_nodes", "_shuffled_ts"):
+                    oc[k] = v
+                elif k in ("sim_bold", "sim_fc_trils", "sim_fcd_trils"):
+                    oc[k] = v[start:end]
+                else:
+                    oc[k] = v[:, start:end]
+            start = end
+            child._process_out(oc)
+
+
+def create_multi_sim_group(sim_group_cls):
+    """MultiSimGroup class for a model's SimGroup (base.py:1440-1461)."""
+    return type("MultiSimGroup", (MultiSimGroupMixin, sim_group_cls), {})
