@@ -73,8 +73,10 @@ struct IntegrateArgs {
     ModelK K;
     int sim_begin;               // first simulation of this launch (FP64 kernel)
     int n_regional;              // regional parameters of the model
-    const int *tiles;            // FP32 kernel: [n_tiles][1 + fp32_tile_sims()] = SC index, then simulation ids (-1 = empty)
+    const int *tiles;            // FP32 kernel: [n_tiles][1 + tile_width] = SC index, then simulation ids (-1 = empty)
     int n_tiles;
+    int tile_width;              // FP32 kernel: simulations per tile (16 or 32)
+    double bw_binom[13];         // FP32 kernel: binomial coefficients C(1/alpha, k), k = 0..12
     int *status;                 // device status word (0 = ok)
 };
 
@@ -104,7 +106,7 @@ struct GofArgs {
 cudaError_t launch_integrate_fp64(int model, const IntegrateArgs &a, cudaStream_t st);
 cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
 bool fp32_supported(int model, int nodes, bool has_delay);
-int fp32_tile_sims();
+int fp32_tile_for(int nodes);  // simulations per FP32 tile for a node count
 cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();

@@ -669,6 +669,14 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     ia.do_fic = c.do_fic; ia.max_fic_trials = c.max_fic_trials; ia.I_start = c.I_start; ia.I_end = c.I_end;
     ia.I_dur = c.I_dur; ia.init_delta = c.init_delta;
     ia.bw = g_bw; ia.bw.dt = c.bw_dt; ia.bw.dt_itau = ia.bw.dt * ia.bw.itau;  // core.cpp:291-292
+    {  // C(1/alpha, k) for the FP32 kernel's binomial form of nu^(1/alpha)
+        long double v = 1.0L;
+        ia.bw_binom[0] = 1.0;
+        for (int k = 1; k <= 12; ++k) {
+            v = v * ((long double)ia.bw.ialpha - (k - 1)) / k;
+            ia.bw_binom[k] = (double)v;
+        }
+    }
     ia.K = make_constants(md.id, c.dt);
     ia.sim_begin = 0;
     ia.n_regional = md.n_regional;
@@ -681,7 +689,8 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
                                                 (c.do_fic && c.max_fic_trials > 0 ? " with numerical FIC" : "") +
                                                 " at " + std::to_string(n) + " nodes; use precision 'fp64'");
         // tiles of simulations that share one SC
-        const int TN = fp32_tile_sims();
+        const int TN = fp32_tile_for(n);
+        ia.tile_width = TN;
         std::vector<int> sc_of(N);
         if (device_io) {
             if (h_sc_idx.size() != (size_t)N) {

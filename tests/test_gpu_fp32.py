@@ -1,0 +1,105 @@
+"""FP32 / tensor-core path against the FP64 path on the same inputs and noise.
+
+Bounds (stated for the mixed-precision mode): |dFC| <= 2e-3 and |dGOF| <= 1e-3
+against the FP64 run of the same seeded noise, for every term.
+All calls go through the C ABI.
+"""
+import numpy as np
+import pytest
+
+import cases
+from cubnm_b200 import core, utils
+
+pytestmark = pytest.mark.gpu
+
+FC_TOL = 2e-3
+GOF_TOL = 1e-3
+
+
+def _pair(args):
+    a64 = [x.copy() if isinstance(x, np.ndarray) else x for x in args]
+    a32 = [x.copy() if isinstance(x, np.ndarray) else x for x in args]
+    a64[7] = dict(args[7], precision="fp64")
+    a32[7] = dict(args[7], precision="fp32")
+    return core.run_simulations(*a64), core.run_simulations(*a32)
+
+
+def _gof_err(o64, o32, nodes, vols, window=10, seed=7):
+    emp = cases.synthetic_emp_bold(nodes, vols, seed)
+    efc = utils.calculate_fc(emp)
+    efcd = utils.calculate_fcd(emp, window, 2)
+    g64 = utils.gof(o64["sim_fc_trils"], efc, o64["sim_fcd_trils"], efcd)
+    g32 = utils.gof(o32["sim_fc_trils"], efc, o32["sim_fcd_trils"], efcd)
+    return {k: float(np.nanmax(np.abs(g64[k] - g32[k]))) for k in g64}
+
+
+def test_rww_readme_grid_within_bounds():
+    """4x5x5 grid over G, w_p, J_N, 100 nodes, 60 s, FC + FCD w10/s2."""
+    G, wp, jn = cases.rww_grid()
+    args = cases.synthetic_args("rWW", N=100, nodes=100, duration_s=60, seed=0, G=G, w_p=wp, J_N=jn)
+    o64, o32 = _pair(args)
+    dfc = np.abs(o64["sim_fc_trils"] - o32["sim_fc_trils"]).max()
+    assert dfc <= FC_TOL, dfc
+    errs = _gof_err(o64, o32, 100, 60)
+    assert max(errs.values()) <= GOF_TOL, errs
+    # BOLD and time-averaged states track closely too
+    assert np.abs(o64["sim_bold"] - o32["sim_bold"]).max() < 1e-3
+    np.testing.assert_allclose(o32["_sim_states"], o64["_sim_states"], rtol=1e-3, atol=1e-3)
+
+
+@pytest.mark.parametrize("model", ["WC", "rWWEx"])
+def test_other_models_within_bounds(model):
+    N, nodes = 32, 68
+    G = np.linspace(0.1, 2.0, N)
+    args = cases.synthetic_args(model, N=N, nodes=nodes, duration_s=40, seed=4, G=G, window_size=10, window_step=2,
+                                bold_remove_s=10)
+    o64, o32 = _pair(args)
+    dfc = np.nanmax(np.abs(o64["sim_fc_trils"] - o32["sim_fc_trils"]))
+    assert dfc <= FC_TOL, dfc
+    errs = _gof_err(o64, o32, nodes, 40)
+    assert max(errs.values()) <= GOF_TOL, errs
+
+
+def test_jr_short_horizon():
+    """Jansen-Rit at these couplings is chaotic: an FP64 run perturbed by 1e-9 diverges
+    exponentially (BOLD difference 1e-11 -> 1e-5 over 40 s), so pointwise FC bounds do not
+    apply over long runs.  Over the first 5 s the FP32 BOLD follows the FP64 BOLD."""
+    N, nodes = 32, 68
+    args = cases.synthetic_args("JR", N=N, nodes=nodes, duration_s=5, seed=4, G=np.linspace(0.1, 2.0, N),
+                                window_size=2, window_step=1, bold_remove_s=1)
+    o64, o32 = _pair(args)
+    scale = np.abs(o64["sim_bold"]).max()
+    assert np.abs(o64["sim_bold"] - o32["sim_bold"]).max() < 1e-4 * scale
+
+
+def test_mixed_sc_tiles_and_partial_tile():
+    """Simulations using three different SCs, interleaved, with N not a multiple of the tile."""
+    N, nodes = 37, 48
+    scs = np.stack([cases.synthetic_sc(nodes, 0.3, s).reshape(-1) for s in range(3)])
+    args = list(cases.synthetic_args("rWW", N=N, nodes=nodes, duration_s=40, seed=2, G=np.linspace(0.5, 4, N),
+                                     bold_remove_s=10))
+    args[1] = scs
+    args[2] = (np.arange(N) % 3).astype(np.intc)
+    o64, o32 = _pair(args)
+    dfc = np.abs(o64["sim_fc_trils"] - o32["sim_fc_trils"]).max()
+    assert dfc <= FC_TOL, dfc
+
+
+def test_unsupported_combinations_are_rejected(golden):
+    args = list(cases.golden_args("rWW", 1, 0, golden=golden))   # with delay
+    args[7] = dict(args[7], precision="fp32")
+    with pytest.raises(RuntimeError, match="fp32"):
+        core.run_simulations(*args)
+    args = list(cases.golden_args("rWW", 0, 2, golden=golden))   # numerical FIC
+    args[7] = dict(args[7], precision="fp32")
+    with pytest.raises(RuntimeError, match="numerical FIC"):
+        core.run_simulations(*args)
+
+
+def test_analytical_fic_in_fp32(golden):
+    """Analytical FIC runs on the host before either integrator: same wIE in both modes."""
+    args = list(cases.golden_args("rWW", 0, 1, N=4, golden=golden))
+    args[4] = np.array([[0.2, 0.5, 1.0, 1.5]])
+    o64, o32 = _pair(args)
+    dfc = np.abs(o64["sim_fc_trils"] - o32["sim_fc_trils"]).max()
+    assert dfc <= FC_TOL, dfc
