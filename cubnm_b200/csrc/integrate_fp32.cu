@@ -126,19 +126,10 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n\t"
-        "tcgen05.wait::ld.sync.aligned;\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-        : "r"(taddr)
-        : "memory");
-}
-
 template <int W>
 __device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[W]) {
-    if constexpr (W == 8) tmem_ld8(taddr, r);
-    else tmem_ld4(taddr, r);
+    static_assert(W == 8, "accumulator reads are 8 columns wide");
+    tmem_ld8(taddr, r);
 }
 
 __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
@@ -188,12 +179,37 @@ __device__ __forceinline__ float rate_fn(float x, float d, float inv_d) {
     return fabsf(y) < 1e-3f ? small : big;
 }
 
+// ---- packed FP32x2 helpers (two simulations per instruction, sm_100 FFMA2 / FADD2 / FMUL2)
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// rate r = x / (1 - exp(-d x)) for a pair; ml2d = -d log2(e).  Near x = 0 the series
+// (1/d)(1 + y/2) (y = d x) replaces the direct form (see rate_fn).
+__device__ __forceinline__ float2 rate2(float2 x, float d, float id, float ml2d) {
+    const float2 t = __fmul2_rn(x, f2(ml2d));
+    const float2 e = make_float2(ex2_approx(t.x), ex2_approx(t.y));
+    const float2 den = __ffma2_rn(e, f2(-1.0f), f2(1.0f));
+    const float2 big = __fmul2_rn(x, make_float2(rcp_approx(den.x), rcp_approx(den.y)));
+    const float2 y = __fmul2_rn(x, f2(d));
+    const float2 small = __fmul2_rn(__ffma2_rn(y, f2(0.5f), f2(1.0f)), f2(id));
+    return make_float2(fabsf(y.x) < 1e-3f ? small.x : big.x, fabsf(y.y) < 1e-3f ? small.y : big.y);
+}
+
 struct RWW32 {  // rww.cpp:194-232 in FP32
-    static constexpr int NP = 5, NS = 2, NN = 2, NOUT = 6;
-    struct K { float wEI0, wII0, aE, bE, dE, idE, aI, bI, dI, idI, wII, dgE, ditE, dgI, ditI, sqdt; };
+    static constexpr int NP = 5, NS = 2, NN = 2, NOUT = 6, CV = 0, BV = 0;
+    struct K { float wEI0, wII0, aE, bE, dE, idE, aI, bI, dI, idI, wII, dgE, ditE, dgI, ditI, sqdt, ml2dE, ml2dI; };
     __device__ static K make(const ModelK &m) {
         const RWWK &r = m.rww;
         K k;
+        k.ml2dE = (float)(-r.d_E * 1.4426950408889634); k.ml2dI = (float)(-r.d_I * 1.4426950408889634);
         k.wEI0 = (float)r.w_E__I_0; k.wII0 = (float)r.w_I__I_0; k.aE = (float)r.a_E; k.bE = (float)r.b_E;
         k.dE = (float)r.d_E; k.idE = (float)(1.0 / r.d_E); k.aI = (float)r.a_I; k.bI = (float)r.b_I;
         k.dI = (float)r.d_I; k.idI = (float)(1.0 / r.d_I); k.wII = (float)r.w_II; k.dgE = (float)r.dt_gamma_E;
@@ -207,21 +223,66 @@ struct RWW32 {  // rww.cpp:194-232 in FP32
         p[4] = (float)r[3] * k.sqdt;
     }
     __device__ static void init(float *s) { s[0] = 0.001f; s[1] = 0.001f; }
-    __device__ static float conn(const float *s) { return s[0]; }
-    __device__ static float bold_in(const float *s) { return s[0]; }
-    __device__ static void step(float *s, const float *p, float in, float n0, float n1, const K &k, float *o) {
-        const float IE = k.wEI0 + p[0] * s[0] + p[1] * in - p[3] * s[1];
-        const float II = k.wII0 + p[2] * s[0] - k.wII * s[1];
-        const float rE = rate_fn(k.aE * IE - k.bE, k.dE, k.idE);
-        const float rI = rate_fn(k.aI * II - k.bI, k.dI, k.idI);
-        s[0] = __saturatef(s[0] + (n0 * p[4] + k.dgE * ((1.0f - s[0]) * rE) - k.ditE * s[0]));
-        s[1] = __saturatef(s[1] + (n1 * p[4] + k.dgI * rI - k.ditI * s[1]));
+    // One Euler step for a pair of simulations, state / params packed as float2 so that
+    // every multiply-add is one FFMA2 (p[3] holds -wIE in this form, see pair_params):
+    //   I_E = wEI0 + w_p J_N S_E + G J_N in - wIE S_I,  I_I = wII0 + J_N S_E - wII S_I,
+    //   S_E += sigma sqrt(dt) n0 + dt gamma_E (1 - S_E) r_E - dt/tau_E S_E   (clamped to [0, 1]),
+    //   S_I += sigma sqrt(dt) n1 + dt gamma_I r_I - dt/tau_I S_I            (clamped to [0, 1]).
+    // Both simulations share the node's noise.
+    static constexpr bool PAIR = true;
+    __device__ static void pair_params(float2 *p) { p[3] = make_float2(-p[3].x, -p[3].y); }
+    __device__ static void step2(float2 *s, const float2 *p, float2 in, float n0, float n1, const K &k, float2 *o) {
+        const float2 sE = s[0], sI = s[1];
+        float2 IE = __ffma2_rn(p[0], sE, f2(k.wEI0));
+        IE = __ffma2_rn(p[1], in, IE);
+        IE = __ffma2_rn(p[3], sI, IE);
+        float2 II = __ffma2_rn(p[2], sE, f2(k.wII0));
+        II = __ffma2_rn(f2(-k.wII), sI, II);
+        const float2 rE = rate2(__ffma2_rn(f2(k.aE), IE, f2(-k.bE)), k.dE, k.idE, k.ml2dE);
+        const float2 rI = rate2(__ffma2_rn(f2(k.aI), II, f2(-k.bI)), k.dI, k.idI, k.ml2dI);
+        float2 dE = __fmul2_rn(f2(n0), p[4]);
+        dE = __ffma2_rn(f2(k.dgE), __fmul2_rn(__ffma2_rn(sE, f2(-1.0f), f2(1.0f)), rE), dE);
+        dE = __ffma2_rn(f2(-k.ditE), sE, dE);
+        float2 dI = __ffma2_rn(f2(k.dgI), rI, __fmul2_rn(f2(n1), p[4]));
+        dI = __ffma2_rn(f2(-k.ditI), sI, dI);
+        const float2 nE = __fadd2_rn(sE, dE), nI = __fadd2_rn(sI, dI);
+        s[0] = make_float2(__saturatef(nE.x), __saturatef(nE.y));
+        s[1] = make_float2(__saturatef(nI.x), __saturatef(nI.y));
         o[0] = IE; o[1] = II; o[2] = rE; o[3] = rI; o[4] = s[0]; o[5] = s[1];
     }
 };
 
+// Pair form for models without a packed step: two scalar steps.
+template <class M, bool = M::PAIR>
+struct PairStep {
+    __device__ static void params(float2 *) {}
+    __device__ static void step(float2 *s, const float2 *p, float2 in, float n0, float n1, const typename M::K &k,
+                                float2 *o) {
+        float sa[M::NS], sb[M::NS], pa[M::NP], pb[M::NP], oa[M::NOUT], ob[M::NOUT];
+#pragma unroll
+        for (int q = 0; q < M::NS; ++q) { sa[q] = s[q].x; sb[q] = s[q].y; }
+#pragma unroll
+        for (int q = 0; q < M::NP; ++q) { pa[q] = p[q].x; pb[q] = p[q].y; }
+        M::step(sa, pa, in.x, n0, n1, k, oa);
+        M::step(sb, pb, in.y, n0, n1, k, ob);
+#pragma unroll
+        for (int q = 0; q < M::NS; ++q) s[q] = make_float2(sa[q], sb[q]);
+#pragma unroll
+        for (int q = 0; q < M::NOUT; ++q) o[q] = make_float2(oa[q], ob[q]);
+    }
+};
+template <class M>
+struct PairStep<M, true> {
+    __device__ static void params(float2 *p) { M::pair_params(p); }
+    __device__ static void step(float2 *s, const float2 *p, float2 in, float n0, float n1, const typename M::K &k,
+                                float2 *o) {
+        M::step2(s, p, in, n0, n1, k, o);
+    }
+};
+
 struct WC32 {  // wc.cpp:51-80 in FP32
-    static constexpr int NP = 9, NS = 2, NN = 2, NOUT = 2;
+    static constexpr bool PAIR = false;
+    static constexpr int NP = 9, NS = 2, NN = 2, NOUT = 2, CV = 0, BV = 0;
     struct K { float dt, sqdt, itE, itI, aE, aI, muE, muI; };
     __device__ static K make(const ModelK &m) {
         const WCK &w = m.wc;
@@ -234,8 +295,6 @@ struct WC32 {  // wc.cpp:51-80 in FP32
         p[8] = (float)G;
     }
     __device__ static void init(float *s) { s[0] = 0.001f; s[1] = 0.001f; }
-    __device__ static float conn(const float *s) { return s[0]; }
-    __device__ static float bold_in(const float *s) { return s[0]; }
     __device__ static void step(float *s, const float *p, float in, float n0, float n1, const K &k, float *o) {
         const float SE = __fdividef(1.0f, 1.0f + __expf(-k.aE * (p[0] * s[0] - p[1] * s[1] + p[8] * in + p[4] - k.muE)));
         const float SI = __fdividef(1.0f, 1.0f + __expf(-k.aI * (p[2] * s[0] - p[3] * s[1] + p[5] - k.muI)));
@@ -248,7 +307,8 @@ struct WC32 {  // wc.cpp:51-80 in FP32
 };
 
 struct RWWEx32 {  // rwwex.cpp:48-73 in FP32
-    static constexpr int NP = 4, NS = 1, NN = 1, NOUT = 3;
+    static constexpr bool PAIR = false;
+    static constexpr int NP = 4, NS = 1, NN = 1, NOUT = 3, CV = 0, BV = 0;
     struct K { float JN, a, b, d, id, dit, dg, sqdt; };
     __device__ static K make(const ModelK &m) {
         const RWWExK &w = m.rwwex;
@@ -259,8 +319,6 @@ struct RWWEx32 {  // rwwex.cpp:48-73 in FP32
         p[0] = (float)(r[0] * k.JN); p[1] = (float)(G * k.JN); p[2] = (float)r[1]; p[3] = (float)r[2] * k.sqdt;
     }
     __device__ static void init(float *s) { s[0] = 0.001f; }
-    __device__ static float conn(const float *s) { return s[0]; }
-    __device__ static float bold_in(const float *s) { return s[0]; }
     __device__ static void step(float *s, const float *p, float in, float n0, float, const K &k, float *o) {
         const float x = p[0] * s[0] + p[1] * in + p[2];
         const float r = rate_fn(k.a * x - k.b, k.d, k.id);
@@ -270,7 +328,8 @@ struct RWWEx32 {  // rwwex.cpp:48-73 in FP32
 };
 
 struct JR32 {  // jr.cpp:80-133 in FP32
-    static constexpr int NP = 7, NS = 8, NN = 1, NOUT = 8;
+    static constexpr bool PAIR = false;
+    static constexpr int NP = 7, NS = 8, NN = 1, NOUT = 8, CV = 7, BV = 6;
     struct K { float dt, sqdt, A, B, a, b, v0, numax2, r, mu, cmin, cmax, mid, asq, bsq; };
     __device__ static K make(const ModelK &m) {
         const JRK &j = m.jr;
@@ -284,8 +343,6 @@ struct JR32 {  // jr.cpp:80-133 in FP32
         p[3] = (float)(r[4] * r[0]); p[4] = (float)r[5] * k.sqdt; p[5] = (float)G; p[6] = 0.0f;
     }
     __device__ static void init(float *s) { for (int i = 0; i < 8; ++i) s[i] = 0.0f; }
-    __device__ static float conn(const float *s) { return s[7]; }
-    __device__ static float bold_in(const float *s) { return s[6]; }
     __device__ static void step(float *s, const float *p, float in, float n0, float, const K &k, float *o) {
         const float s12 = __fdividef(k.numax2, 1.0f + __expf(k.r * (k.v0 - (s[1] - s[2]))));
         const float s01 = __fdividef(k.numax2, 1.0f + __expf(k.r * (k.v0 - p[0] * s[0])));
@@ -429,21 +486,32 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int *td = tiles + (size_t)tile * (TN + 1);
         const int sc_idx = td[0];
+        constexpr int NPR = SPT / 2;
         int sims[SPT];
-        float p[SPT][M::NP];
-        float s[SPT][M::NS];
+        float2 p2[NPR][M::NP];   // parameters of simulation pair (2 pr, 2 pr + 1) of node j
+        float2 s2[NPR][M::NS];   // state of that pair
 #pragma unroll
-        for (int i = 0; i < SPT; ++i) {
-            sims[i] = td[1 + wg * SPT + i];
-            M::init(s[i]);
+        for (int pr = 0; pr < NPR; ++pr) {
+            float pa[2][M::NP], sa[2][M::NS];
 #pragma unroll
-            for (int q = 0; q < M::NP; ++q) p[i][q] = 0.0f;
-            if (act && sims[i] >= 0) {  // parameters of (node j, simulation)
-                double rr[8];
-                for (int q = 0; q < 8; ++q)
-                    rr[q] = q < a.n_regional ? a.rparams[(size_t)q * rstride + (size_t)sims[i] * n + j] : 0.0;
-                M::params(p[i], a.gparams[sims[i]], rr, K);
+            for (int u = 0; u < 2; ++u) {
+                const int i = 2 * pr + u;
+                sims[i] = td[1 + wg * SPT + i];
+                M::init(sa[u]);
+#pragma unroll
+                for (int q = 0; q < M::NP; ++q) pa[u][q] = 0.0f;
+                if (act && sims[i] >= 0) {  // parameters of (node j, simulation)
+                    double rr[8];
+                    for (int q = 0; q < 8; ++q)
+                        rr[q] = q < a.n_regional ? a.rparams[(size_t)q * rstride + (size_t)sims[i] * n + j] : 0.0;
+                    M::params(pa[u], a.gparams[sims[i]], rr, K);
+                }
             }
+#pragma unroll
+            for (int q = 0; q < M::NP; ++q) p2[pr][q] = make_float2(pa[0][q], pa[1][q]);
+#pragma unroll
+            for (int q = 0; q < M::NS; ++q) s2[pr][q] = make_float2(sa[0][q], sa[1][q]);
+            PairStep<M>::params(p2[pr]);
         }
         if (a.ext_out && !a.states_ts && act) {  // states sums start at zero
             for (int i = 0; i < SPT; ++i)
@@ -484,9 +552,9 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
             if (j >= KP) return;
             uint32_t hw[SPT / 2], lw[SPT / 2];
 #pragma unroll
-            for (int i = 0; i < SPT; i += 2) {
-                const float x0 = act ? M::conn(s[i]) : 0.0f, x1 = act ? M::conn(s[i + 1]) : 0.0f;
-                split_bf16x2(x0, x1, hw[i / 2], lw[i / 2]);
+            for (int pr = 0; pr < SPT / 2; ++pr) {
+                const float2 x = act ? s2[pr][M::CV] : make_float2(0.0f, 0.0f);
+                split_bf16x2(x.x, x.y, hw[pr], lw[pr]);
             }
             // simulations n = wg*SPT .. wg*SPT+SPT-1 of the tile
             const int n0 = wg * SPT;
@@ -624,16 +692,23 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                 if (act) {
                     const bool last = sample && (inner == a.inner_it - 1);
 #pragma unroll
-                    for (int i = 0; i < SPT; ++i) {
-                        float o[M::NOUT];
-                        M::step(s[i], p[i], __uint_as_float(acc[i]), n0, n1, K, o);
-                        if (last && sims[i] >= 0) {
-                            if (a.states_ts) {
-                                for (int v = 0; v < M::NOUT; ++v)
-                                    a.states[((size_t)v * a.n_sims + sims[i]) * ext + (size_t)states_i * n + j] = o[v];
-                            } else if (states_i >= a.n_states_samples_remove) {
-                                for (int v = 0; v < M::NOUT; ++v)
-                                    a.states[((size_t)v * a.n_sims + sims[i]) * ext + j] += (double)o[v];
+                    for (int pr = 0; pr < SPT / 2; ++pr) {
+                        float2 o[M::NOUT];
+                        PairStep<M>::step(s2[pr], p2[pr],
+                                          make_float2(__uint_as_float(acc[2 * pr]), __uint_as_float(acc[2 * pr + 1])),
+                                          n0, n1, K, o);
+                        if (last) {
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                const int sim = sims[2 * pr + u];
+                                if (sim < 0) continue;
+                                for (int v = 0; v < M::NOUT; ++v) {
+                                    const double ov = u ? o[v].y : o[v].x;
+                                    if (a.states_ts)
+                                        a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = ov;
+                                    else if (states_i >= a.n_states_samples_remove)
+                                        a.states[((size_t)v * a.n_sims + sim) * ext + j] += ov;
+                                }
                             }
                         }
                     }
@@ -645,7 +720,10 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
             // next bw step's GEMMs
             const bool tr = ((bw_i + 1) % a.bold_tr_iters == 0);
 #pragma unroll
-            for (int i = 0; i < SPT; ++i) zp[i] = M::bold_in(s[i]);
+            for (int pr = 0; pr < SPT / 2; ++pr) {
+                zp[2 * pr] = s2[pr][M::BV].x;
+                zp[2 * pr + 1] = s2[pr][M::BV].y;
+            }
             pend = true;
             pend_tr = tr;
             pend_bi = bold_i;
