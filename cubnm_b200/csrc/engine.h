@@ -111,4 +111,12 @@ cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();
 
+// FC / FCD of device BOLD with the window FCs in a fixed file-scope device
+// array of NOALLOC_SCRATCH_BYTES (fc_noalloc.cu); allocates no device memory.
+// Returns a C-ABI status code and writes a message into msg[cap].
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;
+int fc_fcd_noalloc(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove, int window_size,
+                   int window_step, int drop_edges, int exc_inter, double *fc, double *fcd, cudaStream_t st,
+                   char *msg, size_t cap);
+
 }  // namespace cbnm

@@ -978,4 +978,14 @@ int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc
     });
 }
 
+int cbnm_fc_fcd_noalloc(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove, int window_size,
+                        int window_step, int drop_edges, int exc_interhemispheric, double *fc, double *fcd,
+                        void *stream) {
+    char msg[256];
+    const int rc = fc_fcd_noalloc(bold, n_sims, bold_len, nodes, n_vols_remove, window_size, window_step, drop_edges,
+                                  exc_interhemispheric, fc, fcd, (cudaStream_t)stream, msg, sizeof(msg));
+    g_err = rc ? msg : "";
+    return rc;
+}
+
 }  // extern "C"

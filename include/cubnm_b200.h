@@ -163,6 +163,32 @@ int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc
              const double *sim_fcd, int n_window_pairs, const double *emp_fcd, int n_emp_fcd,
              double *fc_corr, double *fc_diff, double *fc_normec, double *fcd_ks);
 
+/* FC and FCD of simulated BOLD already in device memory, allocating no device
+ * memory.  No counterpart in the reference: there, FC and FCD are computed only
+ * inside run_simulations (src/ext/bnm.cu:809-942).  It is for callers that
+ * cannot allocate on the device: a host whose pooling allocator already holds
+ * the free device memory, or a loop that keeps integration running on other
+ * streams, which the implicit device-wide synchronisation of cudaFree would
+ * stall.
+ *   bold  [n_sims][bold_len*nodes] (device), volume-major per simulation
+ *   fc    [n_sims][n_pairs] (device) -- same values and order as sim_fc_trils
+ *   fcd   [n_sims][n_window_pairs] (device) or NULL for FC only -- as sim_fcd_trils
+ *   n_vols_remove: volumes dropped before FC (bold_remove_s * 1000 / BOLD_TR);
+ *   window_size, window_step, drop_edges, exc_interhemispheric: as in model_config.
+ *   stream: a cudaStream_t (NULL = the default stream); the call only enqueues.
+ * The window FCs of each chunk of simulations go to one fixed device array of
+ * CBNM_NOALLOC_SCRATCH_BYTES per device (32 MiB); a batch whose single
+ * simulation needs more (n_windows * n_pairs * 8 bytes) is rejected with
+ * CBNM_ERR_ARG.  No buffer has to start zeroed.  The scratch is shared, so
+ * calls whose kernels overlap on one device race: serialise them (one stream,
+ * or events).  The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress, with that device current), which can load the module
+ * that holds it; make that first call before any stream capture begins. */
+#define CBNM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int cbnm_fc_fcd_noalloc(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove,
+                        int window_size, int window_step, int drop_edges, int exc_interhemispheric,
+                        double *fc, double *fcd, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
