@@ -105,6 +105,7 @@ struct GofArgs {
 // launchers (return cudaGetLastError() of the launch)
 cudaError_t launch_integrate_fp64(int model, const IntegrateArgs &a, cudaStream_t st);
 cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
+cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStream_t st);  // FP32, one CTA per simulation
 bool fp32_supported(int model, int nodes, bool has_delay);
 int fp32_tile_for(int nodes);  // simulations per FP32 tile for a node count
 cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);

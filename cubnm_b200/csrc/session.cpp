@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -633,7 +634,8 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
         CK(cudaMemcpyAsync(S.d_max_delay.p, h_max_delay.data(), sizeof(int) * N, cudaMemcpyHostToDevice, S.st));
         S.d_hist_off.ensure(sizeof(long long) * N);
         CK(cudaMemcpyAsync(S.d_hist_off.p, h_hist_off.data(), sizeof(long long) * N, cudaMemcpyHostToDevice, S.st));
-        if (c.fp32) S.d_hist_f32.ensure(sizeof(float) * hist_total);
+        // FP32 mode keeps FP32 ring buffers, except for the Kuramoto phase (double)
+        if (c.fp32 && !md.osc) S.d_hist_f32.ensure(sizeof(float) * hist_total);
         else S.d_hist.ensure(sizeof(double) * hist_total);
     }
 
@@ -682,12 +684,27 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     ia.n_regional = md.n_regional;
     ia.status = d_status;
     int launches = 0;
-    if (c.fp32) {
-        if (!fp32_supported(md.id, n, has_delay) || (c.do_fic && c.max_fic_trials > 0))
-            throw Err(CBNM_ERR_UNSUPPORTED, std::string("precision 'fp32' is not available for ") + md.name +
-                                                (has_delay ? " with delay" : "") +
-                                                (c.do_fic && c.max_fic_trials > 0 ? " with numerical FIC" : "") +
-                                                " at " + std::to_string(n) + " nodes; use precision 'fp64'");
+    // The tensor-core tile kernel takes shared-SC batches without delays or
+    // numerical FIC at <= 128 nodes; every other FP32 request runs on the FP32
+    // per-simulation kernel.  CBNM_FP32_KERNEL=simt forces the latter.
+    const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
+    const bool use_tc = c.fp32 && !(fp32_kernel && std::string(fp32_kernel) == "simt") &&
+                        fp32_supported(md.id, n, has_delay) && !(c.do_fic && c.max_fic_trials > 0);
+    if (c.fp32) {  // FP32 SC copy (converted once per run)
+        std::vector<float> f;
+        std::vector<double> tmp;
+        const double *src = h_sc;
+        if (device_io) {
+            tmp.resize(nn * a->n_scs);
+            CK(cudaMemcpy(tmp.data(), a->sc, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+            src = tmp.data();
+        }
+        f.assign(src, src + nn * a->n_scs);
+        S.d_sc_f32.ensure(sizeof(float) * f.size());
+        CK(cudaMemcpyAsync(S.d_sc_f32.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, S.st));
+        ia.sc_f32 = S.d_sc_f32.as<float>();
+    }
+    if (use_tc) {
         // tiles of simulations that share one SC
         const int TN = fp32_tile_for(n);
         ia.tile_width = TN;
@@ -716,22 +733,14 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
         S.d_tiles.ensure(sizeof(int) * tiles.size());
         CK(cudaMemcpyAsync(S.d_tiles.p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, S.st));
         ia.tiles = S.d_tiles.as<int>();
-        // FP32 SC copy (converted once per run)
-        std::vector<float> f;
-        std::vector<double> tmp;
-        const double *src = h_sc;
-        if (device_io) {
-            tmp.resize(nn * a->n_scs);
-            CK(cudaMemcpy(tmp.data(), a->sc, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
-            src = tmp.data();
-        }
-        f.assign(src, src + nn * a->n_scs);
-        S.d_sc_f32.ensure(sizeof(float) * f.size());
-        CK(cudaMemcpyAsync(S.d_sc_f32.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, S.st));
-        ia.sc_f32 = S.d_sc_f32.as<float>();
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));
         CK(launch_integrate_fp32(md.id, ia, S.st, &launches));
+    } else if (c.fp32) {
+        CK(cudaStreamSynchronize(S.st));
+        CK(cudaEventRecord(S.ev[1], S.st));
+        CK(launch_integrate_simt32(md.id, ia, S.st));
+        ++launches;
     } else {
         CK(launch_integrate_fp64(md.id, ia, S.st));
         ++launches;
