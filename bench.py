@@ -158,11 +158,8 @@ def run_ours(opts, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from cubnm_b200.shard import max_over_ranks as shard_max
+        return shard_max(x, device=dev) if dist is not None else x
 
     n_sims = opts.sims
     args = workload_args(n_sims, opts.duration, opts.precision, seed=rank)
