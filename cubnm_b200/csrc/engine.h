@@ -112,6 +112,28 @@ cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();
 
+// Adjoint (reverse-mode) pass of the FP32 rWW integrator + FP64 Balloon-Windkessel
+// model with the noise held fixed (adjoint.cu).  Checkpoints of the state every
+// seg_bw Balloon-Windkessel steps; the backward pass recomputes each segment
+// into a scratch and runs it in reverse.
+struct AdjArgs {
+    IntegrateArgs ia;            // forward arguments (FP32 SC, FP32 noise, BOLD, constants)
+    const float *sct_f32;        // [n_scs][nodes*nodes] transposed SC: sct[a][b] = SC[b][a]
+    int seg_bw, n_seg;           // Balloon-Windkessel steps per segment, segments per simulation
+    float *ck_s;                 // [n_sims][n_seg][2][nodes]  S_E, S_I at each segment start
+    double *ck_bw;               // [n_sims][n_seg][4][nodes]  x, f, nu, q at each segment start
+    const double *dbold;         // [n_sims][bold_len][nodes]  dL/dBOLD
+    float *scr_s;                // [chunk][seg_bw*inner_it][3][nodes]  S_E, S_I, input before each step
+    float *scr_z;                // [chunk][seg_bw][nodes]  Balloon-Windkessel input of each step
+    double *scr_bw;              // [chunk][seg_bw][4][nodes]  Balloon-Windkessel state before each step
+    double *grad_g;              // [1][n_sims]   dL/dG
+    double *grad_r;              // [4][n_sims*nodes]  dL/d(w_p, J_N, wIE, sigma)
+    int sim_begin, sim_count;    // simulations of this launch (backward: the scratch chunk)
+};
+cudaError_t launch_adjoint_forward(const AdjArgs &a, cudaStream_t st);
+cudaError_t launch_adjoint_backward(const AdjArgs &a, cudaStream_t st);
+cudaError_t launch_transpose_sc(const double *sc, float *sc_f32, float *sct_f32, int n_scs, int nodes, cudaStream_t st);
+
 // FC / FCD of device BOLD with the window FCs in a fixed file-scope device
 // array of NOALLOC_SCRATCH_BYTES (fc_noalloc.cu); allocates no device memory.
 // Returns a C-ABI status code and writes a message into msg[cap].

@@ -296,7 +296,7 @@ struct Session {
     // run buffers
     DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
-    DBuf d_tiles;
+    DBuf d_tiles, d_sct_f32;
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -327,7 +327,7 @@ static void release_session() {
         for (DBuf *b : {&S.d_noise, &S.d_noise_f32, &S.d_sh_nodes, &S.d_sh_ts, &S.d_sc, &S.d_sc_f32, &S.d_sc_idx,
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
-                        &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
+                        &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles, &S.d_sct_f32,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -850,6 +850,121 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
 }
 
 // ---------------------------------------------------------------- GOF
+// ---------------------------------------------------------------- adjoint (gradients)
+// Reverse-mode gradient of an FP32 rWW batch (adjoint.cu).  Inputs are device
+// arrays, as cbnm_run_simulations_device; noise and shuffles come from the
+// session cache exactly as for a run with the same seed, nodes and duration.
+struct AdjPlan {
+    Cfg c;
+    const ModelDesc *md = nullptr;
+    int seg_bw = 0, n_seg = 0, chunk = 0;
+    size_t ck_s_bytes = 0, ck_bytes = 0, scr_bw_bytes = 0, scr_s_bytes = 0, scr_z_bytes = 0, scratch_bytes = 0;
+};
+
+static AdjPlan adjoint_plan(const cbnm_run_args *a, int segment_steps) {
+    check_args(a);
+    AdjPlan P;
+    P.md = find_model(a->model_name);
+    if (!P.md) throw Err(CBNM_ERR_MODEL, std::string("Model ") + (a->model_name ? a->model_name : "(null)") + " not found");
+    if (P.md->id != MODEL_RWW) throw Err(CBNM_ERR_UNSUPPORTED, "gradients are implemented for the rWW model only");
+    if (a->do_delay) throw Err(CBNM_ERR_UNSUPPORTED, "gradients with conduction delays are not implemented");
+    if (a->use_cpu) throw Err(CBNM_ERR_UNSUPPORTED, "use_cpu is not supported");
+    build_cfg(P.c, a, *P.md);
+    P.c.fp32 = true;
+    if (P.c.do_fic) throw Err(CBNM_ERR_UNSUPPORTED, "gradients need do_fic = 0 (wIE given)");
+    if (P.c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this build");
+    if (segment_steps <= 0 || segment_steps % P.c.inner_it != 0)
+        throw Err(CBNM_ERR_ARG, "segment_steps must be a positive multiple of bw_dt / dt = " + std::to_string(P.c.inner_it));
+    const int N = P.c.n_sims, n = P.c.nodes;
+    P.seg_bw = segment_steps / P.c.inner_it;
+    P.n_seg = (P.c.bw_it + P.seg_bw - 1) / P.seg_bw;
+    P.ck_s_bytes = sizeof(float) * (size_t)N * P.n_seg * 2 * n;
+    P.ck_bytes = P.ck_s_bytes + sizeof(double) * (size_t)N * P.n_seg * 4 * n;
+    const size_t bw_per = sizeof(double) * (size_t)P.seg_bw * 4 * n;
+    const size_t s_per = sizeof(float) * (size_t)P.seg_bw * P.c.inner_it * 3 * n;
+    const size_t z_per = sizeof(float) * (size_t)P.seg_bw * n;
+    const size_t per_sim = bw_per + s_per + z_per;
+    const size_t budget = (size_t)2 << 30;
+    P.chunk = (int)std::max<size_t>(1, std::min<size_t>(N, budget / per_sim));
+    P.scr_bw_bytes = bw_per * P.chunk;
+    P.scr_s_bytes = s_per * P.chunk;
+    P.scr_z_bytes = z_per * P.chunk;
+    P.scratch_bytes = P.scr_bw_bytes + P.scr_s_bytes + P.scr_z_bytes;
+    return P;
+}
+
+static AdjArgs adjoint_args(Session &S, AdjPlan &P, const cbnm_run_args *a) {
+    const Cfg &c = P.c;
+    ensure_noise(S, c, *P.md, a->force_reinit != 0);
+    const size_t nn = (size_t)c.nodes * c.nodes;
+    S.d_sc_f32.ensure(sizeof(float) * nn * a->n_scs);
+    S.d_sct_f32.ensure(sizeof(float) * nn * a->n_scs);
+    CK(launch_transpose_sc(a->sc, S.d_sc_f32.as<float>(), S.d_sct_f32.as<float>(), a->n_scs, c.nodes, S.st));
+    AdjArgs A;
+    std::memset(&A, 0, sizeof(A));
+    IntegrateArgs &ia = A.ia;
+    ia.nodes = c.nodes; ia.n_sims = c.n_sims; ia.bw_it = c.bw_it; ia.inner_it = c.inner_it;
+    ia.bold_tr_iters = c.bold_tr_iters; ia.noise_bw_it = c.noise_bw_it; ia.bold_len = c.bold_len;
+    ia.sc_f32 = S.d_sc_f32.as<float>(); ia.sc_idx = a->sc_indices;
+    ia.gparams = a->global_params; ia.rparams = a->regional_params;
+    ia.noise_f32 = S.d_noise_f32.as<float>(); ia.sh_nodes = S.d_sh_nodes.as<int>(); ia.sh_ts = S.d_sh_ts.as<int>();
+    ia.bw = g_bw; ia.bw.dt = c.bw_dt; ia.bw.dt_itau = ia.bw.dt * ia.bw.itau;  // core.cpp:291-292
+    ia.K = make_constants(MODEL_RWW, c.dt);
+    A.sct_f32 = S.d_sct_f32.as<float>();
+    A.seg_bw = P.seg_bw; A.n_seg = P.n_seg;
+    return A;
+}
+
+static void adjoint_forward_impl(const cbnm_run_args *a, int segment_steps, double *bold, void *ckpt) {
+    if (!bold || !ckpt) throw Err(CBNM_ERR_ARG, "null bold or checkpoint buffer");
+    AdjPlan P = adjoint_plan(a, segment_steps);
+    Session &S = session();
+    AdjArgs A = adjoint_args(S, P, a);
+    A.ia.bold = bold;
+    A.ck_s = static_cast<float *>(ckpt);
+    A.ck_bw = reinterpret_cast<double *>(static_cast<char *>(ckpt) + P.ck_s_bytes);
+    A.sim_begin = 0; A.sim_count = P.c.n_sims;
+    cbnm_timing tm{};
+    CK(cudaEventRecord(S.ev[0], S.st));
+    CK(launch_adjoint_forward(A, S.st));
+    CK(cudaEventRecord(S.ev[1], S.st));
+    CK(cudaEventSynchronize(S.ev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]));
+    tm.integrate_ms = ms; tm.total_ms = ms; tm.kernel_launches = 2;
+    S.timing = tm;
+}
+
+static void adjoint_backward_impl(const cbnm_run_args *a, int segment_steps, const double *dbold, const void *ckpt,
+                                  void *scratch, double *grad_global, double *grad_regional) {
+    if (!dbold || !ckpt || !scratch || !grad_global || !grad_regional) throw Err(CBNM_ERR_ARG, "null buffer");
+    AdjPlan P = adjoint_plan(a, segment_steps);
+    Session &S = session();
+    AdjArgs A = adjoint_args(S, P, a);
+    A.ck_s = const_cast<float *>(static_cast<const float *>(ckpt));
+    A.ck_bw = reinterpret_cast<double *>(const_cast<char *>(static_cast<const char *>(ckpt)) + P.ck_s_bytes);
+    A.dbold = dbold;
+    A.scr_bw = static_cast<double *>(scratch);
+    A.scr_s = reinterpret_cast<float *>(static_cast<char *>(scratch) + P.scr_bw_bytes);
+    A.scr_z = reinterpret_cast<float *>(static_cast<char *>(scratch) + P.scr_bw_bytes + P.scr_s_bytes);
+    A.grad_g = grad_global; A.grad_r = grad_regional;
+    cbnm_timing tm{};
+    int launches = 1;
+    CK(cudaEventRecord(S.ev[0], S.st));
+    for (int s0 = 0; s0 < P.c.n_sims; s0 += P.chunk) {
+        A.sim_begin = s0;
+        A.sim_count = std::min(P.chunk, P.c.n_sims - s0);
+        CK(launch_adjoint_backward(A, S.st));
+        ++launches;
+    }
+    CK(cudaEventRecord(S.ev[1], S.st));
+    CK(cudaEventSynchronize(S.ev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]));
+    tm.integrate_ms = ms; tm.total_ms = ms; tm.kernel_launches = launches;
+    S.timing = tm;
+}
+
 static void gof_impl(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc, const double *sim_fcd,
                      int n_wp, const double *emp_fcd, int n_emp_fcd, double *fc_corr, double *fc_diff,
                      double *fc_normec, double *fcd_ks) {
@@ -984,6 +1099,29 @@ int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc
     return guarded([&] {
         gof_impl(sim_fc, n_sims, n_pairs, emp_fc, sim_fcd, n_window_pairs, emp_fcd, n_emp_fcd, fc_corr, fc_diff,
                  fc_normec, fcd_ks);
+    });
+}
+
+int cbnm_adjoint_query(const cbnm_run_args *a, int segment_steps, cbnm_adjoint_sizes *sz) {
+    return guarded([&] {
+        if (!sz) throw Err(CBNM_ERR_ARG, "null sizes");
+        AdjPlan P = adjoint_plan(a, segment_steps);
+        sz->n_segments = P.n_seg;
+        sz->checkpoint_bytes = (int64_t)P.ck_bytes;
+        sz->scratch_bytes = (int64_t)P.scratch_bytes;
+        sz->bold_len = P.c.bold_len;
+        sz->sims_per_backward_launch = P.chunk;
+    });
+}
+
+int cbnm_adjoint_forward(const cbnm_run_args *a, int segment_steps, double *bold, void *checkpoints) {
+    return guarded([&] { adjoint_forward_impl(a, segment_steps, bold, checkpoints); });
+}
+
+int cbnm_adjoint_backward(const cbnm_run_args *a, int segment_steps, const double *dbold, const void *checkpoints,
+                          void *scratch, double *grad_global, double *grad_regional) {
+    return guarded([&] {
+        adjoint_backward_impl(a, segment_steps, dbold, checkpoints, scratch, grad_global, grad_regional);
     });
 }
 

@@ -1,0 +1,240 @@
+"""Gradients of a BOLD-based loss with respect to rWW parameters.
+
+The reference fits parameters with grid search and gradient-free optimisers
+(src/cubnm/optimize.py: grid, CMA-ES, NSGA-II over SimGroup.run).  This module
+makes the same simulation differentiable: :class:`RWWProblem` runs a batch of
+rWW simulations through the adjoint entry points of the C ABI
+(``cbnm_adjoint_forward`` / ``cbnm_adjoint_backward``), and
+``RWWProblem.bold(G, w_p, J_N, wIE, sigma)`` returns BOLD as a torch tensor with
+a backward pass, so any torch loss on BOLD yields pathwise gradients (noise held
+fixed) for G per simulation and w_p, J_N, wIE, sigma per node.
+
+The forward is the FP32 per-simulation rWW integrator (FP64 Balloon-Windkessel),
+checkpointed every ``segment_steps`` integration steps; the backward recomputes
+each segment from its checkpoint and runs it in reverse on the GPU.
+
+Losses (FP64 torch, differentiable): :func:`fc_tril`, :func:`fcd_tril`,
+:func:`fc_corr_loss` (1 - Pearson r of FC lower triangles) and
+:func:`fcd_wasserstein` (1-D Wasserstein distance of FCD value distributions
+from sorted values), combined by :func:`rww_fit_loss`.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+
+
+class AdjointSizes(C.Structure):
+    _fields_ = [("n_segments", C.c_int64), ("checkpoint_bytes", C.c_int64), ("scratch_bytes", C.c_int64),
+                ("bold_len", C.c_int64), ("sims_per_backward_launch", C.c_int64)]
+
+
+def _declare(L):
+    if getattr(L, "_adjoint_declared", False):
+        return L
+    vp, ap = C.c_void_p, C.POINTER(_abi.RunArgs)
+    L.cbnm_adjoint_query.argtypes = [ap, C.c_int, C.POINTER(AdjointSizes)]
+    L.cbnm_adjoint_query.restype = C.c_int
+    L.cbnm_adjoint_forward.argtypes = [ap, C.c_int, vp, vp]
+    L.cbnm_adjoint_forward.restype = C.c_int
+    L.cbnm_adjoint_backward.argtypes = [ap, C.c_int, vp, vp, vp, vp, vp]
+    L.cbnm_adjoint_backward.restype = C.c_int
+    L._adjoint_declared = True
+    return L
+
+
+def window_bounds(bold_len, n_vols_remove, window_size, window_step, drop_edges=True):
+    """Inclusive volume ranges of the dynamic-FC windows (src/ext/utils.cpp:21-52)."""
+    corr_len = bold_len - n_vols_remove
+    half = window_size // 2
+    first = (half if drop_edges else 0) + n_vols_remove
+    last = (corr_len - 1 - half if drop_edges else corr_len - 1) + n_vols_remove
+    return [(max(0, c - half), min(bold_len - 1, c + half)) for c in range(first, last + 1, window_step)]
+
+
+def _corr_tril(x):
+    """Pearson r of the columns of x [..., T, n], lower triangle in np.tril_indices(n, -1) order."""
+    import torch
+    xc = x - x.mean(dim=-2, keepdim=True)
+    cov = xc.transpose(-1, -2) @ xc
+    sd = torch.sqrt(torch.diagonal(cov, dim1=-2, dim2=-1))
+    r = cov / (sd.unsqueeze(-1) * sd.unsqueeze(-2))
+    i, j = np.tril_indices(x.shape[-1], -1)
+    return r[..., i, j]
+
+
+def fc_tril(bold, n_vols_remove):
+    """Static FC of BOLD [N, T, n] over volumes [n_vols_remove, T): [N, n_pairs]."""
+    return _corr_tril(bold[:, n_vols_remove:, :])
+
+
+def fcd_tril(bold, n_vols_remove, window_size, window_step, drop_edges=True):
+    """FCD lower triangle of BOLD [N, T, n]: Pearson r between window-FC vectors."""
+    import torch
+    wins = window_bounds(bold.shape[1], n_vols_remove, window_size, window_step, drop_edges)
+    wfc = torch.stack([_corr_tril(bold[:, s:e + 1, :]) for s, e in wins], dim=1)  # [N, W, P]
+    return _corr_tril(wfc.transpose(1, 2))
+
+
+def fc_corr_loss(sim_fc, emp_fc):
+    """1 - Pearson r between each row of sim_fc [N, P] and emp_fc [P]."""
+    import torch
+    s = sim_fc - sim_fc.mean(dim=1, keepdim=True)
+    e = emp_fc - emp_fc.mean()
+    r = (s * e).sum(dim=1) / (torch.sqrt((s * s).sum(dim=1)) * torch.sqrt((e * e).sum()))
+    return 1.0 - r
+
+
+def fcd_wasserstein(sim_fcd, emp_fcd):
+    """1-D Wasserstein distance W1 = int_0^1 |Q_sim(p) - Q_emp(p)| dp between the value
+    distribution of each row of sim_fcd [N, m] and emp_fcd [m2], by the midpoint
+    rule on the simulated quantiles: mean_i |sorted_sim[i] - Q_emp((i + 1/2)/m)|
+    with Q_emp the empirical quantile function (sorted_emp[floor(p m2)]).  Exact
+    when m == m2; the gradient flows through the sorted simulated values."""
+    import torch
+    m, m2 = sim_fcd.shape[1], emp_fcd.numel()
+    emp_sorted = torch.sort(emp_fcd.reshape(-1)).values
+    p = (torch.arange(m, dtype=sim_fcd.dtype, device=sim_fcd.device) + 0.5) / m
+    q = emp_sorted[torch.floor(p * m2).long().clamp(max=m2 - 1)]
+    return (torch.sort(sim_fcd, dim=1).values - q).abs().mean(dim=1)
+
+
+def rww_fit_loss(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges=True):
+    """Per-simulation loss (1 - r(FC)) + W1(FCD) on BOLD [N, T, n]."""
+    return (fc_corr_loss(fc_tril(bold, n_vols_remove), emp_fc) +
+            fcd_wasserstein(fcd_tril(bold, n_vols_remove, window_size, window_step, drop_edges), emp_fcd))
+
+
+class RWWProblem:
+    """A differentiable batch of rWW simulations on one GPU.
+
+    sc: [n_scs, nodes*nodes] or [nodes, nodes] (row = source); sc_indices [N] picks
+    each simulation's SC (all 0 by default).  The noise follows the reference's
+    generator for (sim_seed, nodes, duration, noise segment), exactly as
+    cbnm_run_simulations does, so BOLD equals that of a "fp32" run with the same
+    inputs (per-simulation kernel).
+    """
+
+    def __init__(self, sc, nodes, duration_s, *, sc_indices=None, sim_seed=0, dt=0.1, bw_dt=1.0, bold_tr=1000,
+                 noise_segment_s=30, segment_steps=1000, device="cuda:0"):
+        import torch
+        self.torch = torch
+        self.dev = torch.device(device)
+        self.nodes = int(nodes)
+        sc = np.asarray(sc, dtype=np.float64).reshape(-1, self.nodes * self.nodes)
+        self.sc = torch.from_numpy(np.ascontiguousarray(sc)).to(self.dev)
+        self.sc_indices = None if sc_indices is None else np.asarray(sc_indices, dtype=np.int32)
+        self.duration_ms = int(round(duration_s * 1000))
+        self.sim_seed, self.dt, self.bw_dt, self.bold_tr = int(sim_seed), float(dt), float(bw_dt), int(bold_tr)
+        self.segment_steps = int(segment_steps)
+        self.config = {"do_fc": "0", "do_fcd": "0", "bold_remove_s": "0", "exc_interhemispheric": "0",
+                       "window_size": "10", "window_step": "2", "drop_edges": "1",
+                       "noise_time_steps": str(int(noise_segment_s * 1000)), "verbose": "0",
+                       "progress_interval": "500", "do_fic": "0", "max_fic_trials": "0",
+                       "precision": "fp32"}
+        self.L = _declare(lib())
+        self.last_forward_ms = self.last_backward_ms = 0.0
+
+    def _args(self, N, g, r):
+        """cbnm_run_args for N simulations with device parameter arrays g [1, N], r [4, N*n]."""
+        torch = self.torch
+        n = self.nodes
+        sc_idx = np.zeros(N, np.int32) if self.sc_indices is None else self.sc_indices
+        host = ["rWW", self.sc.cpu().numpy(), sc_idx, np.zeros(n * n), np.zeros((1, N)), np.zeros((4, N * n)),
+                np.zeros(N), self.config, False, False, False, False, False, False, N, n, self.duration_ms,
+                self.bold_tr, self.bold_tr, self.sim_seed, self.dt, self.bw_dt]
+        prep = _abi.Prepared(*host)
+        keep = {"sc_idx": torch.from_numpy(sc_idx).to(self.dev), "dist": torch.zeros(n * n, dtype=torch.float64,
+                                                                                     device=self.dev),
+                "v": torch.zeros(N, dtype=torch.float64, device=self.dev), "g": g, "r": r}
+        dp = lambda x: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+        a = prep.args
+        a.sc = dp(self.sc)
+        a.n_scs = int(self.sc.shape[0])
+        a.sc_indices = C.cast(C.c_void_p(keep["sc_idx"].data_ptr()), C.POINTER(C.c_int32))
+        a.sc_dist = dp(keep["dist"])
+        a.global_params = dp(g)
+        a.regional_params = dp(r)
+        a.v_list = dp(keep["v"])
+        return prep, keep
+
+    def sizes(self, N):
+        torch = self.torch
+        g = torch.zeros((1, N), dtype=torch.float64, device=self.dev)
+        r = torch.zeros((4, N * self.nodes), dtype=torch.float64, device=self.dev)
+        prep, _ = self._args(N, g, r)
+        sz = AdjointSizes()
+        check(self.L.cbnm_adjoint_query(C.byref(prep.args), self.segment_steps, C.byref(sz)))
+        return sz
+
+    def bold(self, G, w_p, J_N, wIE, sigma):
+        """BOLD [N, bold_len, nodes] (float64, on the device) of simulations with G [N]
+        and w_p, J_N, wIE, sigma [N, nodes]; differentiable in all five."""
+        return _BOLD.apply(self, G, w_p, J_N, wIE, sigma)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _load_timing(L):
+    t = _abi.Timing()
+    L.cbnm_last_timing(C.byref(t))
+    return float(t.integrate_ms)
+
+
+def _autograd_function():
+    import torch
+
+    class BOLD(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, prob, G, w_p, J_N, wIE, sigma):
+            N, n = G.shape[0], prob.nodes
+            g = G.detach().to(prob.dev, torch.float64).reshape(1, N).contiguous()
+            r = torch.stack([x.detach().to(prob.dev, torch.float64).reshape(N, n) for x in (w_p, J_N, wIE, sigma)])
+            r = r.reshape(4, N * n).contiguous()
+            prep, keep = prob._args(N, g, r)
+            sz = AdjointSizes()
+            check(prob.L.cbnm_adjoint_query(C.byref(prep.args), prob.segment_steps, C.byref(sz)))
+            bold = torch.empty((N, int(sz.bold_len), n), dtype=torch.float64, device=prob.dev)
+            ckpt = torch.empty(int(sz.checkpoint_bytes), dtype=torch.uint8, device=prob.dev)
+            torch.cuda.synchronize(prob.dev)  # the library runs on its own stream
+            check(prob.L.cbnm_adjoint_forward(C.byref(prep.args), prob.segment_steps, _ptr(bold), _ptr(ckpt)))
+            prob.last_forward_ms = _load_timing(prob.L)
+            ctx.prob, ctx.sz = prob, sz
+            ctx.save_for_backward(g, r, ckpt)
+            return bold
+
+        @staticmethod
+        def backward(ctx, gbold):
+            prob, sz = ctx.prob, ctx.sz
+            g, r, ckpt = ctx.saved_tensors
+            N, n = g.shape[1], prob.nodes
+            gbold = gbold.to(torch.float64).contiguous()
+            scratch = torch.empty(int(sz.scratch_bytes), dtype=torch.uint8, device=prob.dev)
+            gg = torch.empty((1, N), dtype=torch.float64, device=prob.dev)
+            gr = torch.empty((4, N * n), dtype=torch.float64, device=prob.dev)
+            prep, keep = prob._args(N, g, r)
+            torch.cuda.synchronize(prob.dev)
+            check(prob.L.cbnm_adjoint_backward(C.byref(prep.args), prob.segment_steps, _ptr(gbold), _ptr(ckpt),
+                                               _ptr(scratch), _ptr(gg), _ptr(gr)))
+            prob.last_backward_ms = _load_timing(prob.L)
+            gr = gr.reshape(4, N, n)
+            return None, gg[0], gr[0], gr[1], gr[2], gr[3]
+
+    return BOLD
+
+
+class _Lazy:
+    fn = None
+
+    @classmethod
+    def apply(cls, *args):
+        if cls.fn is None:
+            cls.fn = _autograd_function()
+        return cls.fn.apply(*args)
+
+
+_BOLD = _Lazy

@@ -163,6 +163,38 @@ int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc
              const double *sim_fcd, int n_window_pairs, const double *emp_fcd, int n_emp_fcd,
              double *fc_corr, double *fc_diff, double *fc_normec, double *fcd_ks);
 
+/* Gradients (reverse mode) of a loss on BOLD with respect to the rWW parameters,
+ * noise held fixed.  No counterpart in the reference, which fits parameters by
+ * grid search and gradient-free optimisers only (src/cubnm/optimize.py); it
+ * integrates the same model (src/ext/models/rww.cpp:194-232, bnm.cu:117-505).
+ * Scope: model "rWW", no delays, do_fic = 0; the node state is FP32, the
+ * Balloon-Windkessel state FP64 (the "fp32" precision of cbnm_run_simulations,
+ * per-simulation kernel, so the forward BOLD equals that run's BOLD).
+ * All array pointers of args are DEVICE pointers (as cbnm_run_simulations_device).
+ *
+ * 1. cbnm_adjoint_query: sizes of the caller-allocated device buffers.
+ *    segment_steps: integration steps between checkpoints (a multiple of
+ *    bw_dt / dt; 1000 = 0.1 s at dt = 0.1 ms).
+ * 2. cbnm_adjoint_forward: BOLD [n_sims][bold_len][nodes] + checkpoints.
+ * 3. the caller forms dL/dBOLD (same layout) on the device.
+ * 4. cbnm_adjoint_backward: dL/dG -> grad_global [1][n_sims];
+ *    dL/d(w_p, J_N, wIE, sigma) per node -> grad_regional [4][n_sims*nodes].
+ *    Recomputes each segment from its checkpoint into the scratch.
+ * Inputs (SC, parameters, seed, sizes) must be the same in 2 and 4. */
+typedef struct cbnm_adjoint_sizes {
+    int64_t n_segments;               /* checkpoints per simulation */
+    int64_t checkpoint_bytes;         /* device bytes for the checkpoints of all simulations */
+    int64_t scratch_bytes;            /* device bytes of backward scratch */
+    int64_t bold_len;                 /* BOLD volumes per simulation */
+    int64_t sims_per_backward_launch; /* simulations the scratch holds at once */
+} cbnm_adjoint_sizes;
+
+int cbnm_adjoint_query(const cbnm_run_args *args, int segment_steps, cbnm_adjoint_sizes *sizes);
+int cbnm_adjoint_forward(const cbnm_run_args *args, int segment_steps, double *bold, void *checkpoints);
+int cbnm_adjoint_backward(const cbnm_run_args *args, int segment_steps, const double *dbold,
+                          const void *checkpoints, void *scratch, double *grad_global,
+                          double *grad_regional);
+
 /* FC and FCD of simulated BOLD already in device memory, allocating no device
  * memory.  No counterpart in the reference: there, FC and FCD are computed only
  * inside run_simulations (src/ext/bnm.cu:809-942).  It is for callers that
