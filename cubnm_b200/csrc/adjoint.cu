@@ -16,7 +16,8 @@
 //   r(x) = x / (1 - e^{-d x}),  r'(x) = ((1 - e) - d x e) / (1 - e)^2,  e = e^{-d x}
 //   I_E = wEI0 + w_p J_N S_E + G J_N in_j - wIE S_I,   I_I = wII0 + J_N S_E - wII S_I
 //   in_j = sum_k SC[k][j] S_E,k  =>  lambda_S_E,k += sum_j SC[k][j] lambda_in,j  (a transposed product:
-//   node k reads SC^T row k, coalesced across the warp)
+//   node k reads SC^T row k, coalesced across the warp; both products use the
+//   four-accumulator FP32 sum of integrate_sim.cuh)
 // and per millisecond the reverse of the Balloon-Windkessel Euler step
 // (bw.cu:4-15; the f update uses the new x, the q update the new nu) with the
 // BOLD sample (bnm.cpp:316-320) adding dL/dBOLD * dBOLD/d(q, nu).
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(1024) k_adj_forward(const AdjArgs A) {
     const int sim = A.sim_begin + blockIdx.x;
     const int j = threadIdx.x, n = a.nodes;
     const bool act = j < n;
-    extern __shared__ float x1[];
+    extern __shared__ __align__(16) float x1[];
     const float *SC = a.sc_f32 + (size_t)a.sc_idx[sim] * n * n;
     const Params P = load_params(a, sim, j, act);
     float s[M::NS];
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(1024) k_adj_forward(const AdjArgs A) {
             __syncthreads();
             float in = 0.0f;
             if (act) {
-                for (int k = 0; k < n; ++k) in += __ldg(&SC[(size_t)k * n + j]) * x1[k];
+                in = coupling_f32(SC, x1, n, j);
                 fwd_step(s, P, in, a, sh_ts, inner, sh_j);
             }
             __syncthreads();
@@ -138,9 +139,9 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs A) {
     const int sim = A.sim_begin + blockIdx.x;
     const int j = threadIdx.x, n = a.nodes;
     const bool act = j < n;
-    extern __shared__ float sh[];
-    float *x1 = sh;       // S_E of every node (forward recompute)
-    float *lin = sh + n;  // adjoint of every node's coupling input
+    extern __shared__ __align__(16) float sh[];
+    float *x1 = sh;                          // S_E of every node (forward recompute)
+    float *lin = sh + ((n + 3) & ~3);        // adjoint of every node's coupling input (16-byte aligned)
     __shared__ double red[33];
     const float *SC = a.sc_f32 + (size_t)a.sc_idx[sim] * n * n;
     const float *SCT = A.sct_f32 + (size_t)a.sc_idx[sim] * n * n;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs A) {
                 __syncthreads();
                 float in = 0.0f;
                 if (act) {
-                    for (int k = 0; k < n; ++k) in += __ldg(&SC[(size_t)k * n + j]) * x1[k];
+                    in = coupling_f32(SC, x1, n, j);
                     const size_t t = (size_t)b * a.inner_it + inner;
                     scr_s[(t * 3 + 0) * n + j] = s[4];
                     scr_s[(t * 3 + 1) * n + j] = s[5];
@@ -287,9 +288,7 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs A) {
                 }
                 __syncthreads();
                 if (act) {  // lambda_S_E,j += sum_k SC[j][k] lambda_in,k
-                    float acc = 0.0f;
-                    for (int k = 0; k < n; ++k) acc += __ldg(&SCT[(size_t)k * n + j]) * lin[k];
-                    lE += acc;
+                    lE += coupling_f32(SCT, lin, n, j);
                 }
                 __syncthreads();
             }
@@ -327,7 +326,7 @@ cudaError_t launch_adjoint_forward(const AdjArgs &a, cudaStream_t st) {
 
 cudaError_t launch_adjoint_backward(const AdjArgs &a, cudaStream_t st) {
     const int threads = ((a.ia.nodes + 31) / 32) * 32;
-    k_adj_backward<<<a.sim_count, threads, sizeof(float) * 2 * a.ia.nodes, st>>>(a);
+    k_adj_backward<<<a.sim_count, threads, sizeof(float) * 2 * ((a.ia.nodes + 3) & ~3), st>>>(a);
     return cudaGetLastError();
 }
 
