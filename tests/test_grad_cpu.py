@@ -92,3 +92,32 @@ def test_adjoint_query_sizes_and_rejections():
         pa = _abi.Prepared(*a)
         assert L.cbnm_adjoint_query(C.byref(pa.args), seg, C.byref(AdjointSizes())) != 0
         assert L.cbnm_last_error()
+
+
+class _Sphere:
+    """Stand-in for FitProblem: a shifted sphere in the unit box (CPU torch)."""
+
+    def __init__(self, dim):
+        self.torch, self.dev, self.dim, self.evals = torch, torch.device("cpu"), dim, 0
+        self.c = torch.linspace(0.2, 0.8, dim, dtype=torch.float64)
+
+    def loss(self, x):
+        self.evals += x.shape[0]
+        return ((x - self.c) ** 2).sum(dim=1)
+
+    def loss_np(self, x):
+        with torch.no_grad():
+            return self.loss(torch.as_tensor(x, dtype=torch.float64)).numpy()
+
+
+def test_cmaes_and_adam_minimise_a_sphere():
+    from cubnm_b200.fit import adam_fit, cmaes_fit, grid_fit, time_to
+    hist, x = cmaes_fit(_Sphere(12), popsize=16, generations=120, seed=1)
+    assert hist[-1][1] < 1e-6 and all(b1 >= b2 for (_, b1), (_, b2) in zip(hist, hist[1:]))
+    np.testing.assert_allclose(x, np.linspace(0.2, 0.8, 12), atol=2e-3)
+    hist, x = adam_fit(_Sphere(12), n_starts=4, iters=300, lr=0.05)
+    assert hist[-1][1] < 1e-4
+    s = _Sphere(3)
+    s.nodes = 1
+    hist, x = grid_fit(s, 5)
+    assert hist[-1][1] <= 0.1 and time_to(hist, 1e9) is not None
