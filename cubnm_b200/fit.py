@@ -79,7 +79,7 @@ class FitProblem:
         return np.where(np.isfinite(v), v, np.inf)
 
 
-def adam_fit(fp, n_starts, iters, lr=0.1, seed=0):
+def adam_fit(fp, n_starts, iters, lr=0.6, seed=0):
     """Adam from n_starts random starts (one batch); returns the history
     [(seconds, best loss so far)] and the best unit-box point."""
     torch = fp.torch
@@ -191,27 +191,32 @@ def main(argv=None):
     ap.add_argument("--step", type=int, default=5)
     ap.add_argument("--popsize", type=int, default=128)
     ap.add_argument("--generations", type=int, default=40)
-    ap.add_argument("--adam-iters", type=int, default=20)
-    ap.add_argument("--lr", type=float, default=0.1)
+    ap.add_argument("--adam-iters", type=int, default=14)
+    ap.add_argument("--lr", type=float, default=0.6)
     ap.add_argument("--grid", type=int, default=6)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--methods", default="grid,cmaes,adam", help="comma-separated subset of grid,cmaes,adam")
+    ap.add_argument("--target", type=float, default=None, help="loss to time against (default: CMA-ES's best)")
     o = ap.parse_args(argv)
     sc = synthetic_sc(o.nodes, 0.25, o.seed)
     emp = synthetic_emp_bold(o.nodes, o.duration, o.seed + 7)
     fp = FitProblem(sc, emp, o.duration, window_size=o.window, window_step=o.step)
     fp.loss_np(np.full((2, fp.dim), 0.5))  # warm-up: noise generation, allocations
     res = {}
+    methods = o.methods.split(",")
     for name, fn in (("grid", lambda: grid_fit(fp, o.grid)),
                      ("cmaes", lambda: cmaes_fit(fp, o.popsize, o.generations, seed=o.seed)),
                      ("adam", lambda: adam_fit(fp, o.popsize, o.adam_iters, lr=o.lr, seed=o.seed))):
+        if name not in methods:
+            continue
         fp.evals = 0
         hist, _ = fn()
         res[name] = {"best": hist[-1][1], "seconds": hist[-1][0], "simulations": fp.evals,
                      "history": [[round(t, 3), b] for t, b in hist]}
-    target = res["cmaes"]["best"]
-    res["target_cmaes_best"] = target
-    res["seconds_to_cmaes_best"] = {k: time_to([tuple(h) for h in res[k]["history"]], target)
-                                    for k in ("grid", "cmaes", "adam")}
+    target = o.target if o.target is not None else res["cmaes"]["best"]
+    res["target"] = target
+    res["seconds_to_target"] = {k: time_to([tuple(h) for h in res[k]["history"]], target) for k in res
+                                if k in ("grid", "cmaes", "adam")}
     res["config"] = vars(o)
     print(json.dumps(res))
 
