@@ -78,6 +78,14 @@ struct IntegrateArgs {
     int tile_width;              // FP32 kernel: simulations per tile (16 or 32)
     double bw_binom[13];         // FP32 kernel: binomial coefficients C(1/alpha, k), k = 0..12
     int *status;                 // device status word (0 = ok)
+    // Sparse coupling (per-simulation kernels), ELLPACK by target node: entry q of
+    // node j at [q * nodes + j]; ell_k entries per node, zero-weight padding last.
+    int ell_k;                   // 0 = dense coupling
+    int n_delay_tables;
+    const int *ell_idx;          // [n_scs][ell_k][nodes] source node
+    const double *ell_w;         // [n_scs][ell_k][nodes] SC weight (FP64 kernel)
+    const float *ell_w32;        // [n_scs][ell_k][nodes] SC weight (FP32 kernel)
+    const int *ell_delay;        // [n_scs][n_delay_tables][ell_k][nodes] delay in steps (with delays)
 };
 
 // FC / FCD (reference: src/ext/fc.cu, src/ext/fc.cpp).

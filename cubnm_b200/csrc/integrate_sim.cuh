@@ -33,12 +33,14 @@ struct SimArrays<double> {
     __device__ static const double *sc(const IntegrateArgs &a) { return a.sc; }
     __device__ static const double *noise(const IntegrateArgs &a) { return a.noise; }
     __device__ static double *hist(const IntegrateArgs &a) { return a.hist; }
+    __device__ static const double *ell_w(const IntegrateArgs &a) { return a.ell_w; }
 };
 template <>
 struct SimArrays<float> {
     __device__ static const float *sc(const IntegrateArgs &a) { return a.sc_f32; }
     __device__ static const float *noise(const IntegrateArgs &a) { return a.noise_f32; }
     __device__ static float *hist(const IntegrateArgs &a) { return a.hist_f32; }
+    __device__ static const float *ell_w(const IntegrateArgs &a) { return a.ell_w32; }
 };
 
 // FP32 coupling input of node j, sum_k SC[k][j] x[k] (x in shared memory, 16-byte
@@ -60,7 +62,7 @@ __device__ __forceinline__ float coupling_f32(const float *__restrict__ SC, cons
     return (s0 + s1) + (s2 + s3);
 }
 
-template <class M, bool DELAY, class R>
+template <class M, bool DELAY, class R, bool SPARSE>
 __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     const int sim = a.sim_begin + blockIdx.x;
     const int j = threadIdx.x;
@@ -72,7 +74,12 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     S *x1 = reinterpret_cast<S *>(smem_raw);  // conn-state of every node, previous step (no delay)
     __shared__ int s_trial, s_adjust, s_failed;
 
-    const R *SC = SimArrays<R>::sc(a) + (size_t)a.sc_idx[sim] * n * n;
+    const int sc_i = a.sc_idx[sim];
+    const R *SC = SimArrays<R>::sc(a) + (size_t)sc_i * n * n;
+    // sparse coupling: the nonzero sources of node j (ascending k), then zero-weight padding
+    const int EK = SPARSE ? a.ell_k : 0;
+    const int *e_idx = SPARSE ? a.ell_idx + (size_t)sc_i * EK * n : nullptr;
+    const R *e_w = SPARSE ? SimArrays<R>::ell_w(a) + (size_t)sc_i * EK * n : nullptr;
     const R *noise = SimArrays<R>::noise(a);
     R g[M::NG], iv[M::NI];
     P r[M::NR];
@@ -96,10 +103,12 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     int D = 0, buff = 0;
     S *hist = nullptr;
     const int *dly = nullptr;
+    const int *e_dly = nullptr;
     if (DELAY) {
         D = a.max_delay[sim];
         hist = SimArrays<S>::hist(a) + a.hist_off[sim];
         dly = a.delay + (size_t)a.delay_idx[sim] * n * n;
+        if (SPARSE) e_dly = a.ell_delay + ((size_t)sc_i * a.n_delay_tables + a.delay_idx[sim]) * EK * n;
         buff = D - 1;
     }
     auto reset_conn = [&]() {
@@ -119,7 +128,26 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
             __syncthreads();  // conn-states of the previous step are visible
             R in = R(0);
             if (act) {
-                if (DELAY) {
+                if (SPARSE && DELAY) {
+                    const S xj = hist[(size_t)buff * n + j];
+                    for (int q = 0; q < EK; ++q) {
+                        const size_t e = (size_t)q * n + j;
+                        const int k = __ldg(&e_idx[e]);
+                        int kb = buff + __ldg(&e_dly[e]);
+                        if (kb >= D) kb -= D;
+                        const S xk = hist[(size_t)kb * n + k];
+                        if (M::OSC) in += __ldg(&e_w[e]) * sin(R(xk - xj));
+                        else in += __ldg(&e_w[e]) * R(xk);
+                    }
+                } else if (SPARSE) {
+                    const S xj = x1[j];
+                    for (int q = 0; q < EK; ++q) {
+                        const size_t e = (size_t)q * n + j;
+                        const S xk = x1[__ldg(&e_idx[e])];
+                        if (M::OSC) in += __ldg(&e_w[e]) * sin(R(xk - xj));
+                        else in += __ldg(&e_w[e]) * R(xk);
+                    }
+                } else if (DELAY) {
                     const S xj = hist[(size_t)buff * n + j];
                     for (int k = 0; k < n; ++k) {
                         int kb = buff + __ldg(&dly[(size_t)k * n + j]);
@@ -245,8 +273,14 @@ template <class M, class R>
 cudaError_t launch_sim_kernel(const IntegrateArgs &a, cudaStream_t st) {
     const int threads = ((a.nodes + 31) / 32) * 32;
     const size_t smem = a.has_delay ? 0 : sizeof(typename M::S) * a.nodes;
-    if (a.has_delay) k_integrate_sim<M, true, R><<<a.n_sims - a.sim_begin, threads, smem, st>>>(a);
-    else k_integrate_sim<M, false, R><<<a.n_sims - a.sim_begin, threads, smem, st>>>(a);
+    const int grid = a.n_sims - a.sim_begin;
+    if (a.ell_k > 0) {
+        if (a.has_delay) k_integrate_sim<M, true, R, true><<<grid, threads, smem, st>>>(a);
+        else k_integrate_sim<M, false, R, true><<<grid, threads, smem, st>>>(a);
+    } else {
+        if (a.has_delay) k_integrate_sim<M, true, R, false><<<grid, threads, smem, st>>>(a);
+        else k_integrate_sim<M, false, R, false><<<grid, threads, smem, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
