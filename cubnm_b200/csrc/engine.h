@@ -116,6 +116,17 @@ cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_
 cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStream_t st);  // FP32, one CTA per simulation
 bool fp32_supported(int model, int nodes, bool has_delay);
 int fp32_tile_for(int nodes);  // simulations per FP32 tile for a node count
+// rWW analytical FIC (fic.cu): wIE written into regional row 2 in place.
+struct FicArgs {
+    int nodes, n_sims;
+    const double *sc;            // [n_scs][nodes*nodes]
+    const int *sc_idx;           // [n_sims]
+    const double *gparams;       // [1][n_sims] G
+    double *regional;            // [n_regional][n_sims*nodes] (w_p, J_N read; wIE written)
+    unsigned char *unstable;     // [n_sims] 1 where FIC failed (wIE set to 1)
+    RWWK K;
+};
+cudaError_t launch_rww_fic(const FicArgs &a, cudaStream_t st);
 cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();

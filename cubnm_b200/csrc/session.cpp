@@ -381,94 +381,6 @@ static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool for
     }
 }
 
-// ---------------------------------------------------------------- analytical FIC
-// Brent's method (Brent 1973; Numerical Recipes zbrent form) driven through
-// GSL's documented fsolver protocol: each iteration reports the bracket, the
-// caller stops when |hi-lo| < 1e-3 * min(|lo|,|hi|) (0 if the bracket holds 0),
-// at most 100 iterations, -1 on failure (rww_fic.cpp:62-102).
-template <class F>
-static double brent_root(F f, double x_lo, double x_hi) {
-    const double eps = 2.2204460492503131e-16;
-    double a = x_lo, b = x_hi, fa = f(a), fb = f(b);
-    if ((fa < 0.0 && fb < 0.0) || (fa > 0.0 && fb > 0.0)) return -1;
-    double c = b, fc = fb, d = b - a, e = b - a, root = 0.5 * (x_lo + x_hi);
-    for (int iter = 1; iter <= 100; ++iter) {
-        bool lin = false;
-        if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) { lin = true; c = a; fc = fa; d = b - a; e = b - a; }
-        if (std::fabs(fc) < std::fabs(fb)) { lin = true; a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
-        const double tol = 0.5 * eps * std::fabs(b), m = 0.5 * (c - b);
-        double lo, hi;
-        if (fb == 0) {
-            root = b; lo = b; hi = b;
-        } else if (std::fabs(m) <= tol) {
-            root = b; lo = std::min(b, c); hi = std::max(b, c);
-        } else {
-            if (std::fabs(e) < tol || std::fabs(fa) <= std::fabs(fb)) {
-                d = m; e = m;
-            } else {
-                double p, q, r, s = fb / fa;
-                if (lin) { p = 2 * m * s; q = 1 - s; }
-                else {
-                    q = fa / fc; r = fb / fc;
-                    p = s * (2 * m * q * (q - r) - (b - a) * (r - 1));
-                    q = (q - 1) * (r - 1) * (s - 1);
-                }
-                if (p > 0) q = -q; else p = -p;
-                if (2 * p < std::min(3 * m * q - std::fabs(tol * q), std::fabs(e * q))) { e = d; d = p / q; }
-                else { d = m; e = m; }
-            }
-            a = b; fa = fb;
-            if (std::fabs(d) > tol) b += d; else b += (m > 0 ? +tol : -tol);
-            fb = f(b);
-            root = b;
-            double cc = c;
-            if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) cc = a;
-            if (b < cc) { lo = b; hi = cc; } else { lo = cc; hi = b; }
-        }
-        const double alo = std::fabs(lo), ahi = std::fabs(hi);
-        const double min_abs = ((lo > 0 && hi > 0) || (lo < 0 && hi < 0)) ? std::min(alo, ahi) : 0.0;
-        if (std::fabs(hi - lo) < 0.001 * min_abs) return root;
-    }
-    return -1;
-}
-
-// rww.cpp:73-146 + rww_fic.cpp:138-231; regional [n_r][N*n] host array, in/out.
-static void rww_analytical_fic(const Cfg &c, const cbnm_run_args *a, const double *gparams, double *regional,
-                               uint8_t *unstable, const RWWK &m) {
-    const int n = c.nodes;
-    const size_t stride = (size_t)c.n_sims * n;
-    const double I0_I = m.I_0 * m.w_I, I0_E = m.I_0 * m.w_E;
-    const double a_I = 615, b_I = 177, d_I = 0.087;  // rww.cpp:19-21
-    auto phi_I = [&](double II) { return ((a_I * II) - b_I) / (1 - std::exp(-1 * d_I * ((a_I * II) - b_I))); };
-    std::vector<double> w_IE(n);
-    for (int sim = 0; sim < c.n_sims; ++sim) {
-        const double *sc = a->sc + (size_t)a->sc_indices[sim] * n * n;
-        const double G = gparams[sim];
-        bool bad = false;
-        for (int j = 0; j < n && !bad; ++j) {
-            const double w_EI_j = regional[1 * stride + (size_t)sim * n + j];
-            const double w_EE_j = regional[0 * stride + (size_t)sim * n + j] * w_EI_j;
-            auto F = [&](double x) { return I0_I + w_EI_j * m.S_E_ss - m.w_II * m.gamma_I_s * m.tau_I_s * phi_I(x) - x; };
-            const double I_I = brent_root(F, 0.0, 2.0);
-            if (I_I == -1) { bad = true; break; }
-            const double r_I = phi_I(I_I);
-            const double S_I_ss = r_I * m.tau_I_s * m.gamma_I_s;
-            double dot = 0.0;
-            for (int k = 0; k < n; ++k) {
-                double kee = (sc[(size_t)k * n + j] * G) * w_EI_j;  // K_EE[j][k], SC transposed
-                if (k == j) kee = kee + w_EE_j;
-                dot += kee * m.S_E_ss;
-            }
-            const double w = (-1 / S_I_ss) * (m.I_E_ss - m.I_ext - I0_E - dot);
-            if (w < 0) { bad = true; break; }
-            w_IE[j] = w;
-        }
-        unstable[sim] = bad ? 1 : 0;
-        if (bad) std::fprintf(stderr, "In simulation #%d analytical FIC failed. Setting wIE to 1 in all nodes\n", sim);
-        for (int j = 0; j < n; ++j) regional[2 * stride + (size_t)sim * n + j] = bad ? 1.0 : w_IE[j];
-    }
-}
-
 // ---------------------------------------------------------------- helpers
 static double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -551,19 +463,6 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
         tm.h2d_bytes += sizeof(double) * nn * a->n_scs + sizeof(int) * N;
         h_g.assign(a->global_params, a->global_params + gsize);
         h_r.assign(a->regional_params, a->regional_params + rsize);
-    }
-    if (c.do_fic) {  // analytical FIC on the host (rww.cpp:73-146)
-        cbnm_run_args ha = *a;
-        std::vector<double> h_sc_copy;
-        if (device_io) {
-            h_sc_copy.resize(nn * a->n_scs);
-            CK(cudaMemcpy(h_sc_copy.data(), a->sc, sizeof(double) * nn * a->n_scs, cudaMemcpyDeviceToHost));
-            ha.sc = h_sc_copy.data();
-            ha.sc_indices = h_sc_idx.data();
-        }
-        rww_analytical_fic(c, &ha, h_g.data(), h_r.data(), h_gbools.data(), make_constants(MODEL_RWW, c.dt).rww);
-        if (device_io)
-            CK(cudaMemcpyAsync(a->regional_params, h_r.data(), sizeof(double) * rsize, cudaMemcpyHostToDevice, S.st));
     }
     if (!device_io) {
         S.d_g.ensure(sizeof(double) * gsize);
@@ -653,6 +552,15 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     int *d_status = (int *)S.d_status.ensure(sizeof(int));
     CK(cudaMemsetAsync(d_status, 0, sizeof(int), S.st));
     CK(cudaEventRecord(S.ev[1], S.st));
+
+    // ---- analytical FIC on the GPU (rww.cpp:73-146): wIE into the regional
+    // parameters in place, failure flags into global_bools[0]
+    if (c.do_fic) {
+        FicArgs fa;
+        fa.nodes = n; fa.n_sims = N; fa.sc = d_sc; fa.sc_idx = d_sc_idx; fa.gparams = d_g; fa.regional = d_r;
+        fa.unstable = d_gbools; fa.K = make_constants(MODEL_RWW, c.dt).rww;
+        CK(launch_rww_fic(fa, S.st));
+    }
 
     // ---- integrate
     IntegrateArgs ia;
@@ -893,6 +801,12 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     CK(cudaStreamSynchronize(S.st));
     if (h_status != 0)
         throw Err(CBNM_ERR_TIMEOUT, "a device-side wait in the integrator gave up (status " + std::to_string(h_status) + ")");
+    if (c.do_fic) {  // report every simulation whose analytical FIC failed, as prep_params does (rww.cpp:73-146)
+        std::vector<uint8_t> flags(N);
+        CK(cudaMemcpy(flags.data(), d_gbools, N, cudaMemcpyDeviceToHost));
+        for (int s2 = 0; s2 < N; ++s2)
+            if (flags[s2]) std::fprintf(stderr, "In simulation #%d analytical FIC failed. Setting wIE to 1 in all nodes\n", s2);
+    }
     if (a->noise_out) {  // core.cpp:429-435
         if (device_io) {
             CK(cudaMemcpy(o->noise, S.d_noise.p, sizeof(double) * S.noise.size(), cudaMemcpyDeviceToDevice));

@@ -105,6 +105,27 @@ def test_fp64_matches_oracle_fic_and_delay(golden):
     _assert_close(ga[5], oa[5], "written-back regional params (wIE)")
 
 
+def test_gpu_analytical_fic_matches_oracle():
+    """Analytical FIC runs on the GPU (one thread per node, the Brent iteration of
+    the host code); wIE and the failure flags equal the oracle's host FIC, including
+    simulations where it fails: with J_N < -1.62 the steady-state equation has no
+    root in [0, 2], and the simulation gets wIE = 1 in every node."""
+    N, nodes = 48, 68
+    rng = np.random.default_rng(9)
+    J_N = np.concatenate([rng.uniform(0.001, 0.5, N - 6), np.full(6, -2.0)])
+    args = list(cases.synthetic_args("rWW", N=N, nodes=nodes, duration_s=2, seed=9, G=np.linspace(0.001, 10, N),
+                                     w_p=rng.uniform(0, 2, N), J_N=J_N, do_fic=1, do_fc=False, do_fcd=False,
+                                     bold_remove_s=0))
+    ga = [a.copy() if isinstance(a, np.ndarray) else a for a in args]
+    oa = [a.copy() if isinstance(a, np.ndarray) else a for a in args]
+    o_gpu = core.run_simulations(*ga)
+    o_cpu = oracle.run_simulations(*oa)
+    np.testing.assert_array_equal(o_gpu["_global_bools"][0], o_cpu["_global_bools"][0])
+    assert o_cpu["_global_bools"][0].sum() >= 1 and o_cpu["_global_bools"][0].sum() < N
+    np.testing.assert_allclose(ga[5][2], oa[5][2], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(o_gpu["sim_bold"], o_cpu["sim_bold"], rtol=1e-8, atol=1e-12)
+
+
 def test_fp64_kuramoto_matches_oracle():
     N, nodes = 3, 32
     args = list(cases.synthetic_args("Kuramoto", N=N, nodes=nodes, duration_s=12, G=np.array([0.2, 1.0, 4.0]),
