@@ -127,6 +127,8 @@ struct FicArgs {
     RWWK K;
 };
 cudaError_t launch_rww_fic(const FicArgs &a, cudaStream_t st);
+// Normal noise from Philox4x32-10 + Box-Muller (noise.cu); out32 may be null.
+cudaError_t launch_philox_normals(uint32_t seed, double *out, float *out32, size_t count, cudaStream_t st);
 cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();

@@ -132,6 +132,7 @@ struct Cfg {
     int I_start = 1000, I_end = 10000, I_dur = 10000 - 1000 + 1;
     double init_delta = 0.02;
     bool fp32 = false;
+    bool philox = false;  // noise segment from Philox on the GPU instead of the host mt19937
     int nodes = 0, n_sims = 0, time_steps = 0, bold_tr = 0, states_sampling = 0, sim_seed = 0;
     double dt = 0.1, bw_dt = 0.001;
     int bold_len = 0, bold_tr_iters = 0, states_len = 0, states_sampling_iters = 0, bw_it = 0, inner_it = 0;
@@ -173,6 +174,10 @@ static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
             if (v == "fp32") c.fp32 = true;
             else if (v == "fp64") c.fp32 = false;
             else throw Err(CBNM_ERR_CONFIG, "precision must be 'fp64' or 'fp32', got '" + v + "'");
+        } else if (k == "noise") {
+            if (v == "philox") c.philox = true;
+            else if (v == "mt19937") c.philox = false;
+            else throw Err(CBNM_ERR_CONFIG, "noise must be 'mt19937' or 'philox', got '" + v + "'");
         }
         if (md.id == MODEL_RWW) {
             if (k == "do_fic") c.do_fic = to_int(k, v) != 0;
@@ -289,6 +294,8 @@ struct Session {
     // noise cache (bnm.cu:1207-1215 key)
     bool noise_valid = false, noise_f32_valid = false;
     int k_seed = 0, k_time = 0, k_nodes = 0, k_nts = 0, k_nnoise = 0;
+    bool k_philox = false;
+    size_t noise_n = 0;  // values in the noise segment (on the host too unless Philox)
     double k_bwdt = 0, k_dt = 0;
     std::vector<double> noise;
     std::vector<int> sh_nodes, sh_ts;
@@ -340,12 +347,18 @@ static void release_session() {
 static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool force) {
     const bool same = S.noise_valid && S.k_seed == c.sim_seed && S.k_time == c.time_steps && S.k_nodes == c.nodes &&
                       S.k_nts == c.noise_time_steps && S.k_nnoise == md.n_noise && S.k_bwdt == c.bw_dt &&
-                      S.k_dt == c.dt;
+                      S.k_dt == c.dt && S.k_philox == c.philox;
     if (!same || force) {
         std::mt19937 gen(c.sim_seed);
-        std::normal_distribution<double> nd(0, 1);
-        S.noise.resize((size_t)c.noise_size);
-        for (int64_t i = 0; i < c.noise_size; ++i) S.noise[i] = nd(gen);
+        S.noise_n = (size_t)c.noise_size;
+        if (c.philox) {  // the segment is drawn on the GPU below; the shuffles from mt19937(seed)
+            S.noise.clear();
+            S.noise.shrink_to_fit();
+        } else {
+            std::normal_distribution<double> nd(0, 1);
+            S.noise.resize(S.noise_n);
+            for (int64_t i = 0; i < c.noise_size; ++i) S.noise[i] = nd(gen);
+        }
         std::vector<int> idx(c.nodes);
         S.sh_nodes.resize((size_t)c.noise_repeats * c.nodes);
         std::iota(idx.begin(), idx.end(), 0);
@@ -360,8 +373,11 @@ static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool for
             shuffle_positions(ts, gen);
             std::copy(ts.begin(), ts.end(), S.sh_ts.begin() + (size_t)r * c.noise_bw_it);
         }
-        S.d_noise.ensure(sizeof(double) * S.noise.size());
-        CK(cudaMemcpyAsync(S.d_noise.p, S.noise.data(), sizeof(double) * S.noise.size(), cudaMemcpyHostToDevice, S.st));
+        S.d_noise.ensure(sizeof(double) * S.noise_n);
+        if (c.philox)
+            CK(launch_philox_normals((uint32_t)c.sim_seed, S.d_noise.as<double>(), nullptr, S.noise_n, S.st));
+        else
+            CK(cudaMemcpyAsync(S.d_noise.p, S.noise.data(), sizeof(double) * S.noise_n, cudaMemcpyHostToDevice, S.st));
         S.d_sh_nodes.ensure(sizeof(int) * S.sh_nodes.size());
         CK(cudaMemcpyAsync(S.d_sh_nodes.p, S.sh_nodes.data(), sizeof(int) * S.sh_nodes.size(), cudaMemcpyHostToDevice, S.st));
         S.d_sh_ts.ensure(sizeof(int) * S.sh_ts.size());
@@ -370,7 +386,14 @@ static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool for
         S.noise_valid = true;
         S.noise_f32_valid = false;
         S.k_seed = c.sim_seed; S.k_time = c.time_steps; S.k_nodes = c.nodes; S.k_nts = c.noise_time_steps;
-        S.k_nnoise = md.n_noise; S.k_bwdt = c.bw_dt; S.k_dt = c.dt;
+        S.k_nnoise = md.n_noise; S.k_bwdt = c.bw_dt; S.k_dt = c.dt; S.k_philox = c.philox;
+    }
+    if (c.fp32 && !S.noise_f32_valid && c.philox) {  // regenerate, writing both copies
+        S.d_noise_f32.ensure(sizeof(float) * S.noise_n);
+        CK(launch_philox_normals((uint32_t)c.sim_seed, S.d_noise.as<double>(), S.d_noise_f32.as<float>(), S.noise_n,
+                                 S.st));
+        CK(cudaStreamSynchronize(S.st));
+        S.noise_f32_valid = true;
     }
     if (c.fp32 && !S.noise_f32_valid) {
         std::vector<float> f(S.noise.begin(), S.noise.end());
@@ -809,11 +832,12 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     }
     if (a->noise_out) {  // core.cpp:429-435
         if (device_io) {
-            CK(cudaMemcpy(o->noise, S.d_noise.p, sizeof(double) * S.noise.size(), cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(o->noise, S.d_noise.p, sizeof(double) * S.noise_n, cudaMemcpyDeviceToDevice));
             CK(cudaMemcpy(o->shuffled_nodes, S.d_sh_nodes.p, sizeof(int) * S.sh_nodes.size(), cudaMemcpyDeviceToDevice));
             CK(cudaMemcpy(o->shuffled_ts, S.d_sh_ts.p, sizeof(int) * S.sh_ts.size(), cudaMemcpyDeviceToDevice));
         } else {
-            std::memcpy(o->noise, S.noise.data(), sizeof(double) * S.noise.size());
+            if (S.noise.size() == S.noise_n) std::memcpy(o->noise, S.noise.data(), sizeof(double) * S.noise_n);
+            else CK(cudaMemcpy(o->noise, S.d_noise.p, sizeof(double) * S.noise_n, cudaMemcpyDeviceToHost));
             std::memcpy(o->shuffled_nodes, S.sh_nodes.data(), sizeof(int) * S.sh_nodes.size());
             std::memcpy(o->shuffled_ts, S.sh_ts.data(), sizeof(int) * S.sh_ts.size());
         }
