@@ -41,8 +41,8 @@ N_SIMS = 32768
 NODES = 100
 DURATION_S = 60
 # dram__bytes_read.sum + dram__bytes_write.sum of one integrator launch of the default
-# workload, from a one-pass ncu capture of the full-size run (5,835 MB + 3,929 MB);
-# the command and the per-kernel table are in profiles/launches_rww_32768x60s_fp32.md
+# workload (5,835 MB + 3,929 MB), measured by ncu with those one-pass metrics on the
+# full-size run (python bench.py --steps 1 --warmup 0 --skip-fp64 --skip-cpu)
 TRAFFIC_DEFAULT_WORKLOAD = 9.7639e9
 WORKLOAD = f"rWW {NODES} nodes, {N_SIMS} sims, {DURATION_S} s, dt 0.1 ms, TR 1 s, FC+FCD w10/s2"
 METRIC = "rWW sims x sim-s per wall-s (100 nodes, 32k sims)"
@@ -245,7 +245,7 @@ def run_ours(opts, rank, world, local_rank):
     issued = 3 * 2.0 * 128 * (((NODES + 15) // 16) * 16) * (n_sims * 1.0) * (opts.duration * 1e4)  # BF16x3 MMA work
     traffic, traffic_src = opts.traffic, "--traffic" if opts.traffic is not None else None
     if traffic is None and n_sims == N_SIMS and opts.duration == DURATION_S and opts.precision == "fp32":
-        traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, "ncu one-pass capture of this workload (profiles/)"
+        traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, "ncu one-pass capture of this full-size workload"
     roof = {"bound": "tensor", "achieved": useful / integ / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
             "frac": useful / integ / 1e12 / peak_tf,
             "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else "fallback",
