@@ -13,7 +13,11 @@
 //    issued as tcgen05.mma kind::f16 with A = SC^T held in TMEM (BF16, written
 //    once per SC) and B = x in shared memory (BF16, MN-major, rewritten every
 //    step), in BF16x3 split precision: D = A_hi B_hi + A_hi B_lo + A_lo B_hi,
-//    FP32 accumulation in TMEM.  Keeping A in TMEM leaves only the 16-column x
+//    FP32 accumulation in TMEM.  The three passes are issued by three threads
+//    (lane 0 of warps 0..2) into three accumulator sets that the readers add:
+//    one thread issuing all 21 MMAs of a step was itself a bottleneck (the
+//    three-issuer form measured 8% faster; a fourth issuer no further gain, as
+//    the tensor pipe then bounds the GEMM).  Keeping A in TMEM leaves only the 16-column x
 //    slice to be read from shared memory per MMA.  Elementwise model updates run
 //    in FP32 registers.
 //  * The Balloon-Windkessel state (bnm.cu:357-371) stays FP64 and lives in TMEM
@@ -23,7 +27,7 @@
 //  * Every wait on the MMA barrier is bounded; on timeout the CTA records a
 //    status, leaves its loop, frees its TMEM and returns.
 //
-// TMEM columns: [0, NACC TN) accumulator sets | [TN, TN + KP) SC^T hi then lo, two BF16
+// TMEM columns: [0, NACC TN) accumulator sets | [NACC TN, NACC TN + KP) SC^T hi then lo, two BF16
 // per column, K chunk kk at +8kk | [COLS - 8 TN, COLS) Balloon-Windkessel state.
 // SMEM B operand (MN-major, no swizzle, 8-row x 16-byte core matrices):
 //   element (k, n) at (k/8)*LBO_B + (n/8)*128 + (k%8)*16 + (n%8)*2,
@@ -53,6 +57,9 @@ struct Tile {
     static constexpr int TMEM_COLS = (COL_BW + TN * 8 <= 256) ? 256 : 512;
     static constexpr int CTAS_PER_SM = 512 / TMEM_COLS;
     static constexpr uint32_t LBO_B = (TN / 8) * 128;
+    // threads that issue the step's GEMM: 1 (all MMAs, round-robin over the NACC sets)
+    // or NACC (thread p of warp p issues pass p of BF16x3 into accumulator set p)
+    static constexpr int ISSUERS = (NACC == 3) ? 3 : 1;
 };
 constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL;  // about 2 s at 1.9 GHz
 
@@ -458,7 +465,8 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm->mbar)), "r"(1));
+        // one arrival per issuing thread (ISSUERS of them commit each step)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm->mbar)), "r"(T::ISSUERS));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         sm->abort = 0;
         sm->sc_loaded = -1;
@@ -631,8 +639,24 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                 fence_before();
                 __syncthreads();
                 if (sm->abort) { aborted = true; break; }
-                // (2) one thread issues the BF16x3 coupling GEMM (A from TMEM, B from SMEM)
-                if (tid == 0) {
+                // (2) the BF16x3 coupling GEMM (A from TMEM, B from SMEM)
+                if constexpr (T::ISSUERS == 3) {
+                    // three issuing threads in three warps, one BF16x3 pass each, into
+                    // accumulator sets 0..2; each commits its own MMAs to the barrier
+                    if ((tid & 31) == 0 && warp < 3) {
+                        fence_after();
+                        const int pass = warp;
+                        const uint32_t bh = smem_u32(B_hi), bl = smem_u32(B_lo);
+                        const uint32_t d = tmem + COL_ACC + pass * TN;
+                        const int nk = KP / 16;
+                        for (int kk = 0; kk < nk; ++kk) {
+                            const uint32_t ta = tmem + COL_A + (pass == 2 ? half : 0) + kk * 8;
+                            const uint64_t db = smem_desc((pass == 1 ? bl : bh) + kk * 2 * LBO_B, LBO_B, 128);
+                            mma_bf16_ts(d, ta, db, idesc, kk > 0 ? 1u : 0u);
+                        }
+                        mma_commit(mbar);
+                    }
+                } else if (tid == 0) {
                     fence_after();
                     const uint32_t bh = smem_u32(B_hi), bl = smem_u32(B_lo);
                     const int nk = KP / 16;
@@ -754,7 +778,7 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
 }
 
 using Tile16 = Tile<16, 8, 1>;   // 2 warpgroups x 8 simulations, two CTAs per SM
-using Tile32 = Tile<32, 8, 1>;   // 4 warpgroups x 8 simulations, one CTA per SM
+using Tile32 = Tile<32, 8, 3>;   // 4 warpgroups x 8 simulations, one CTA per SM, 3 GEMM issuers
 
 template <class T>
 size_t smem_bytes(int KP) { return (size_t)2 * KP * T::TN * 2 + sizeof(Smem) + 64; }
