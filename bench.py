@@ -41,9 +41,9 @@ N_SIMS = 32768
 NODES = 100
 DURATION_S = 60
 # dram__bytes_read.sum + dram__bytes_write.sum of one integrator launch of the default
-# workload (5,835 MB + 3,929 MB), measured by ncu with those one-pass metrics on the
+# workload (9,673 MB + 4,926 MB), measured by ncu with those one-pass metrics on the
 # full-size run (python bench.py --steps 1 --warmup 0 --skip-fp64 --skip-cpu)
-TRAFFIC_DEFAULT_WORKLOAD = 9.7639e9
+TRAFFIC_DEFAULT_WORKLOAD = 14.5994e9
 WORKLOAD = f"rWW {NODES} nodes, {N_SIMS} sims, {DURATION_S} s, dt 0.1 ms, TR 1 s, FC+FCD w10/s2"
 METRIC = "rWW sims x sim-s per wall-s (100 nodes, 32k sims)"
 UNIT = "sims*sim-s/s"
