@@ -158,51 +158,83 @@ class Prepared:
         self.noise_out = bool(noise_out)
 
 
+class _Pending:
+    """One run's C structs and the numpy outputs they point into."""
+
+    def __init__(self, lib, prefix, args):
+        self.p = p = Prepared(*args)
+        self.sizes = sizes = Sizes()
+        st = getattr(lib, prefix + "query_sizes")(C.byref(p.args), C.byref(sizes))
+        if st != 0:
+            raise RuntimeError(getattr(lib, prefix + "last_error")().decode())
+        N, n = p.N, p.nodes
+        self.bold = np.empty((N, sizes.bold_len * n), dtype=np.float64)
+        self.fc = np.empty((N, sizes.n_pairs), dtype=np.float64) if sizes.do_fc else None
+        self.fcd = np.empty((N, sizes.n_window_pairs), dtype=np.float64) if sizes.do_fcd else None
+        ext = n * (sizes.states_len if p.states_ts else 1)
+        self.states = np.empty((sizes.n_state_vars, N, ext), dtype=np.float64) if p.ext_out else None
+        self.gbools = np.zeros((sizes.n_global_out_bool, N), dtype=np.uint8)
+        self.gints = np.zeros((sizes.n_global_out_int, N), dtype=np.int32)
+        self.noise = self.sh_nodes = self.sh_ts = None
+        if p.noise_out:
+            self.noise = np.empty(sizes.noise_size, dtype=np.float64)
+            self.sh_nodes = np.empty((sizes.noise_repeats, n), dtype=np.int32)
+            self.sh_ts = np.empty((sizes.noise_repeats, sizes.noise_bw_it), dtype=np.int32)
+        self.out = Outputs(
+            _ptr(self.bold, C.c_double), _ptr(self.fc, C.c_double), _ptr(self.fcd, C.c_double),
+            _ptr(self.states, C.c_double), _ptr(self.gbools, C.c_uint8), _ptr(self.gints, C.c_int32),
+            _ptr(self.noise, C.c_double), _ptr(self.sh_nodes, C.c_int32), _ptr(self.sh_ts, C.c_int32), 0.0, 0.0,
+        )
+
+    def result(self, wall):
+        out, sizes, p = self.out, self.sizes, self.p
+        res = {
+            "init_time": float(out.init_time),
+            "run_time": float(out.run_time) if out.run_time > 0 else wall,
+            "sim_bold": self.bold,
+        }
+        if sizes.do_fc:
+            res["sim_fc_trils"] = self.fc
+            if sizes.do_fcd:
+                res["sim_fcd_trils"] = self.fcd
+        if p.ext_out:
+            res["_sim_states"] = self.states
+            res["_global_bools"] = self.gbools.astype(bool)
+            res["_global_ints"] = self.gints
+        if p.noise_out:
+            res["_noise"] = self.noise
+            res["_shuffled_nodes"] = self.sh_nodes
+            res["_shuffled_ts"] = self.sh_ts
+        return res
+
+
 def run(lib, prefix, *args):
     """Calls ``<prefix>run_simulations`` and returns the reference's output dict."""
-    p = Prepared(*args)
-    sizes = Sizes()
-    st = getattr(lib, prefix + "query_sizes")(C.byref(p.args), C.byref(sizes))
-    if st != 0:
-        raise RuntimeError(getattr(lib, prefix + "last_error")().decode())
-    N, n = p.N, p.nodes
-    bold = np.empty((N, sizes.bold_len * n), dtype=np.float64)
-    fc = np.empty((N, sizes.n_pairs), dtype=np.float64) if sizes.do_fc else None
-    fcd = np.empty((N, sizes.n_window_pairs), dtype=np.float64) if sizes.do_fcd else None
-    ext = n * (sizes.states_len if p.states_ts else 1)
-    states = np.empty((sizes.n_state_vars, N, ext), dtype=np.float64) if p.ext_out else None
-    gbools = np.zeros((sizes.n_global_out_bool, N), dtype=np.uint8)
-    gints = np.zeros((sizes.n_global_out_int, N), dtype=np.int32)
-    noise = sh_nodes = sh_ts = None
-    if p.noise_out:
-        noise = np.empty(sizes.noise_size, dtype=np.float64)
-        sh_nodes = np.empty((sizes.noise_repeats, n), dtype=np.int32)
-        sh_ts = np.empty((sizes.noise_repeats, sizes.noise_bw_it), dtype=np.int32)
-    out = Outputs(
-        _ptr(bold, C.c_double), _ptr(fc, C.c_double), _ptr(fcd, C.c_double), _ptr(states, C.c_double),
-        _ptr(gbools, C.c_uint8), _ptr(gints, C.c_int32), _ptr(noise, C.c_double),
-        _ptr(sh_nodes, C.c_int32), _ptr(sh_ts, C.c_int32), 0.0, 0.0,
-    )
+    pend = _Pending(lib, prefix, args)
     t0 = time.perf_counter()
-    st = getattr(lib, prefix + "run_simulations")(C.byref(p.args), C.byref(out))
+    st = getattr(lib, prefix + "run_simulations")(C.byref(pend.p.args), C.byref(pend.out))
     t1 = time.perf_counter()
     if st != 0:
         raise RuntimeError(getattr(lib, prefix + "last_error")().decode())
-    res = {
-        "init_time": float(out.init_time),
-        "run_time": float(out.run_time) if out.run_time > 0 else t1 - t0,
-        "sim_bold": bold,
-    }
-    if sizes.do_fc:
-        res["sim_fc_trils"] = fc
-        if sizes.do_fcd:
-            res["sim_fcd_trils"] = fcd
-    if p.ext_out:
-        res["_sim_states"] = states
-        res["_global_bools"] = gbools.astype(bool)
-        res["_global_ints"] = gints
-    if p.noise_out:
-        res["_noise"] = noise
-        res["_shuffled_nodes"] = sh_nodes
-        res["_shuffled_ts"] = sh_ts
-    return res
+    return pend.result(t1 - t0)
+
+
+def run_batch(lib, groups):
+    """Calls ``cbnm_run_batch`` on a list of 22-argument tuples; returns one
+    output dict per group (the same dicts as :func:`run`)."""
+    pends = [_Pending(lib, "cbnm_", g) for g in groups]
+    n = len(pends)
+    args = (RunArgs * n)(*[q.p.args for q in pends])
+    outs = (Outputs * n)(*[q.out for q in pends])
+    statuses = (C.c_int * n)()
+    f = lib.cbnm_run_batch
+    f.argtypes = [C.POINTER(RunArgs), C.POINTER(Outputs), C.c_int, C.POINTER(C.c_int)]
+    f.restype = C.c_int
+    t0 = time.perf_counter()
+    st = f(args, outs, n, statuses)
+    t1 = time.perf_counter()
+    if st != 0:
+        raise RuntimeError(lib.cbnm_last_error().decode())
+    for i, q in enumerate(pends):  # the library filled the structs of the array (init / run times)
+        q.out = outs[i]
+    return [q.result(t1 - t0) for q in pends]

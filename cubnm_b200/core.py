@@ -51,6 +51,19 @@ def run_simulations(*args):
         raise
 
 
+def run_batch(groups):
+    """Runs several independent groups concurrently on the GPU: ``groups`` is a list
+    of 22-argument tuples exactly as for :func:`run_simulations`; returns one
+    output dict per group.  Groups may differ in model, node count, duration,
+    delays and precision; the outputs equal those of separate calls, and modified
+    parameters (rWW FIC) are written back into each group's own arrays."""
+    groups = [tuple(g) for g in groups]
+    for g in groups:
+        if len(g) != 22:
+            raise TypeError("every group needs the 22 run_simulations arguments")
+    return _abi.run_batch(lib(), groups)
+
+
 def last_timing():
     """CUDA-event timings (ms) and transfer sizes of the last run."""
     t = _abi.Timing()

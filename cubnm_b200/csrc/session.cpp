@@ -21,6 +21,8 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 #include <cuda_runtime.h>
 
@@ -310,38 +312,49 @@ struct Session {
     ~Session() {}
 };
 static Session *g_sess = nullptr;
+static std::vector<Session *> g_batch;  // one per concurrent worker of cbnm_run_batch
+static cbnm_timing g_last_timing{};     // timings of the last run call (single, batch or adjoint)
+
+static void open_session(Session &S) {
+    if (S.ready) return;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: no CUDA device available (") + cudaGetErrorString(e) + ")");
+    CK(cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking));
+    for (auto &ev : S.ev) CK(cudaEventCreate(&ev));
+    S.ready = true;
+}
 
 static Session &session() {
     if (!g_sess) g_sess = new Session();
-    Session &S = *g_sess;
-    if (!S.ready) {
-        int ndev = 0;
-        cudaError_t e = cudaGetDeviceCount(&ndev);
-        if (e != cudaSuccess || ndev == 0)
-            throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: no CUDA device available (") + cudaGetErrorString(e) + ")");
-        CK(cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking));
-        for (auto &ev : S.ev) CK(cudaEventCreate(&ev));
-        S.ready = true;
-    }
-    return S;
+    open_session(*g_sess);
+    return *g_sess;
 }
 
-static void release_session() {
-    if (!g_sess) return;
-    Session &S = *g_sess;
+static void close_session(Session *&p) {
+    if (!p) return;
+    Session &S = *p;
     if (S.ready) {
         cudaStreamSynchronize(S.st);
         for (DBuf *b : {&S.d_noise, &S.d_noise_f32, &S.d_sh_nodes, &S.d_sh_ts, &S.d_sc, &S.d_sc_f32, &S.d_sc_idx,
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
-                        &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles, &S.d_sct_f32, &S.d_ell_idx, &S.d_ell_w, &S.d_ell_w32, &S.d_ell_delay,
+                        &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
+                        &S.d_sct_f32, &S.d_ell_idx, &S.d_ell_w, &S.d_ell_w32, &S.d_ell_delay,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
         cudaStreamDestroy(S.st);
     }
-    delete g_sess;
-    g_sess = nullptr;
+    delete p;
+    p = nullptr;
+}
+
+static void release_session() {
+    close_session(g_sess);
+    for (Session *&b : g_batch) close_session(b);
+    g_batch.clear();
 }
 
 static void ensure_noise(Session &S, const Cfg &c, const ModelDesc &md, bool force) {
@@ -427,7 +440,9 @@ static void fill_sizes(const Cfg &c, const ModelDesc &md, cbnm_sizes *sz) {
 }
 
 // ---------------------------------------------------------------- run
-static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
+// sp: the session to run on; null = the process's default session, opened once
+// the arguments have been validated (so argument errors come before device errors)
+static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     const double t_begin = now_s();
     check_args(a);
     if (!o || !o->sim_bold) throw Err(CBNM_ERR_ARG, "null output arrays");
@@ -447,7 +462,7 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     for (int s = 0; s < c.n_sims && !device_io; ++s)
         if (a->sc_indices[s] < 0 || a->sc_indices[s] >= a->n_scs) throw Err(CBNM_ERR_ARG, "SC index out of range");
 
-    Session &S = session();
+    Session &S = sp ? *sp : session();
     cbnm_timing tm{};
     const int N = c.n_sims, n = c.nodes;
     const size_t nn = (size_t)n * n, gsize = (size_t)md.n_global * N, rsize = (size_t)md.n_regional * N * n;
@@ -850,6 +865,7 @@ static void run_impl(const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[4])); tm.total_ms = ms;
     tm.kernel_launches = launches;
     S.timing = tm;
+    g_last_timing = tm;
     o->init_time = init_time;
     o->run_time = now_s() - t_begin - init_time;
 }
@@ -938,6 +954,7 @@ static void adjoint_forward_impl(const cbnm_run_args *a, int segment_steps, doub
     CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]));
     tm.integrate_ms = ms; tm.total_ms = ms; tm.kernel_launches = 2;
     S.timing = tm;
+    g_last_timing = tm;
 }
 
 static void adjoint_backward_impl(const cbnm_run_args *a, int segment_steps, const double *dbold, const void *ckpt,
@@ -968,6 +985,7 @@ static void adjoint_backward_impl(const cbnm_run_args *a, int segment_steps, con
     CK(cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]));
     tm.integrate_ms = ms; tm.total_ms = ms; tm.kernel_launches = launches;
     S.timing = tm;
+    g_last_timing = tm;
 }
 
 static void gof_impl(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc, const double *sim_fcd,
@@ -1078,17 +1096,74 @@ int cbnm_query_sizes(const cbnm_run_args *a, cbnm_sizes *sz) {
 }
 
 int cbnm_run_simulations(const cbnm_run_args *a, cbnm_outputs *o) {
-    return guarded([&] { run_impl(a, o, false); });
+    return guarded([&] { run_impl(nullptr, a, o, false); });
 }
 
 int cbnm_run_simulations_device(const cbnm_run_args *a, cbnm_outputs *o) {
-    return guarded([&] { run_impl(a, o, true); });
+    return guarded([&] { run_impl(nullptr, a, o, true); });
+}
+
+// Groups run concurrently, each worker on its own session (stream, buffers, noise
+// cache): up to 16 host threads, worker w taking groups w, w + K, w + 2K, .. so a
+// repeated batch finds each group's noise cached in the same session.
+int cbnm_run_batch(const cbnm_run_args *args, cbnm_outputs *outs, int n_groups, int *statuses) {
+    return guarded([&] {
+        if (!args || !outs || n_groups < 1) throw Err(CBNM_ERR_ARG, "null batch or no groups");
+        const int K = std::min(n_groups, 16);
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        while ((int)g_batch.size() < K) g_batch.push_back(new Session());
+        for (int w = 0; w < K; ++w) open_session(*g_batch[w]);
+        std::vector<int> codes(n_groups, CBNM_OK);
+        std::vector<std::string> errs(n_groups);
+        std::atomic<int> launches{0};
+        std::atomic<long long> h2d{0}, d2h{0};
+        const double t0 = now_s();
+        auto worker = [&](int w) {
+            const cudaError_t e = cudaSetDevice(dev);
+            for (int g = w; g < n_groups; g += K) {
+                if (e != cudaSuccess) {
+                    codes[g] = CBNM_ERR_CUDA;
+                    errs[g] = std::string("CUDA Error: ") + cudaGetErrorString(e);
+                    continue;
+                }
+                try {
+                    run_impl(g_batch[w], &args[g], &outs[g], false);
+                    const cbnm_timing &t = g_batch[w]->timing;
+                    launches += t.kernel_launches;
+                    h2d += t.h2d_bytes;
+                    d2h += t.d2h_bytes;
+                } catch (const Err &x) {
+                    codes[g] = x.code;
+                    errs[g] = x.what();
+                } catch (const std::exception &x) {
+                    codes[g] = CBNM_ERR_CONFIG;
+                    errs[g] = x.what();
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int w = 0; w < K; ++w) pool.emplace_back(worker, w);
+        for (auto &t : pool) t.join();
+        cbnm_timing tm{};
+        tm.total_ms = (now_s() - t0) * 1e3;
+        for (int w = 0; w < K; ++w) {
+            tm.integrate_ms = std::max(tm.integrate_ms, g_batch[w]->timing.integrate_ms);
+            tm.fc_ms = std::max(tm.fc_ms, g_batch[w]->timing.fc_ms);
+        }
+        tm.kernel_launches = launches.load();
+        tm.h2d_bytes = h2d.load();
+        tm.d2h_bytes = d2h.load();
+        g_last_timing = tm;
+        if (statuses) std::copy(codes.begin(), codes.end(), statuses);
+        for (int g = 0; g < n_groups; ++g)
+            if (codes[g] != CBNM_OK) throw Err(codes[g], "group " + std::to_string(g) + ": " + errs[g]);
+    });
 }
 
 int cbnm_last_timing(cbnm_timing *t) {
     if (!t) return CBNM_ERR_ARG;
-    if (g_sess) *t = g_sess->timing;
-    else std::memset(t, 0, sizeof(*t));
+    *t = g_last_timing;
     return CBNM_OK;
 }
 

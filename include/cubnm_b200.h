@@ -141,7 +141,22 @@ int cbnm_run_simulations(const cbnm_run_args *args, cbnm_outputs *out);
  * No reference counterpart: it is the device-resident form of core.cpp:194-493. */
 int cbnm_run_simulations_device(const cbnm_run_args *args, cbnm_outputs *out);
 
-/* Timings of the last cbnm_run_simulations[_device] call. */
+/* Several independent runs ("groups": each a full cbnm_run_simulations call with
+ * HOST buffers, possibly of different models, node counts, durations, delays and
+ * precisions) executed concurrently.  No counterpart in the reference, whose
+ * interface runs one group per call (src/ext/core.cpp:194-493); a group of a
+ * few hundred small networks fills only part of a B200, so running the groups
+ * of an uneven batch side by side fills it.  Up to 16 groups run at once, each
+ * on its own stream with its own device buffers and noise cache (kept across
+ * calls, freed by cbnm_reset).  Outputs equal those of separate
+ * cbnm_run_simulations calls.  statuses (optional, [n_groups]) receives each
+ * group's status; the return value is the first failing group's status (0 if
+ * none) and cbnm_last_error() names that group. */
+int cbnm_run_batch(const cbnm_run_args *args, cbnm_outputs *outs, int n_groups, int *statuses);
+
+/* Timings of the last cbnm_run_simulations[_device] / cbnm_run_batch /
+ * cbnm_adjoint_* call (for a batch: wall time in total_ms, the longest group's
+ * kernel times, summed transfer sizes and launches). */
 int cbnm_last_timing(cbnm_timing *timing);
 
 /* Drops the cached session (device buffers and noise); core.cpp keeps it for
