@@ -14,7 +14,9 @@ e2e   : the same through the host C-ABI entry (cbnm_run_simulations with host
         buffers: parameters and SC copied in, BOLD/FC/FCD/states copied out)
         plus the GOF scoring call, timed on the host.
 fp64  : the FP64 reference-precision path, measured on a 4,736-simulation
-        subset (a full GPU wave), for the precision/speed comparison.
+        subset (a full GPU wave), for the precision/speed comparison; beside it
+        the FP32 path on the same subset, without and (end to end) with the
+        reference's default analytical FIC.
 
 --impl reference times the reference's own CPU algorithm (the oracle
 restatement, OpenMP over simulations, all host threads) on a bounded sample.
@@ -228,8 +230,18 @@ def run_ours(opts, rank, world, local_rank):
         fp32_sub = workload_args(n64, opts.duration, opts.precision, seed=rank)
         core.run_simulations(*fp32_sub)
         t32 = core.last_timing()
+        # the same subset with the reference's default rWW setting, analytical FIC on
+        # (wIE solved per node on the GPU before the integrator), end to end
+        fic_sub = workload_args(n64, opts.duration, opts.precision, seed=rank)
+        fic_sub[7] = dict(fic_sub[7], do_fic="1")
+        fic_sub[5][2] = 0.0
+        core.run_simulations(*[a.copy() if isinstance(a, np.ndarray) else a for a in fic_sub])
+        t0 = time.perf_counter()
+        core.run_simulations(*fic_sub)
+        t_fic = time.perf_counter() - t0
         fp64 = {"value": n64 * opts.duration / ((t64["integrate_ms"] + t64["fc_ms"]) / 1e3),
                 "fp32_same_subset": n64 * opts.duration / ((t32["integrate_ms"] + t32["fc_ms"]) / 1e3),
+                "fp32_same_subset_fic_e2e": n64 * opts.duration / t_fic,
                 "sims": n64, "unit": UNIT}
 
     # roofline of the dominant kernel (the integrator): coupling on the tensor pipe
