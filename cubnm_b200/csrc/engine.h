@@ -80,12 +80,13 @@ struct IntegrateArgs {
     int *status;                 // device status word (0 = ok)
     // Sparse coupling (per-simulation kernels), ELLPACK by target node: entry q of
     // node j at [q * nodes + j]; ell_k entries per node, zero-weight padding last.
+    // One entry = the SC weight packed with the source's offset into the ring
+    // buffer, d * nodes + k (d = delay in steps of the pair k -> j; without
+    // delays d = 0 and the offset is the source node k), read by one vector load.
     int ell_k;                   // 0 = dense coupling
-    int n_delay_tables;
-    const int *ell_idx;          // [n_scs][ell_k][nodes] source node
-    const double *ell_w;         // [n_scs][ell_k][nodes] SC weight (FP64 kernel)
-    const float *ell_w32;        // [n_scs][ell_k][nodes] SC weight (FP32 kernel)
-    const int *ell_delay;        // [n_scs][n_delay_tables][ell_k][nodes] delay in steps (with delays)
+    int ell_tables;              // delay tables packed per SC (1 without delays)
+    const int2 *ell_pk32;        // [n_scs][ell_tables][ell_k][nodes] {offset, float weight bits} (FP32 kernel)
+    const int4 *ell_pk64;        // [n_scs][ell_tables][ell_k][nodes] {weight lo, weight hi, offset, 0} (FP64 kernel)
 };
 
 // FC / FCD (reference: src/ext/fc.cu, src/ext/fc.cpp).

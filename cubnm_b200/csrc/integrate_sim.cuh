@@ -33,14 +33,20 @@ struct SimArrays<double> {
     __device__ static const double *sc(const IntegrateArgs &a) { return a.sc; }
     __device__ static const double *noise(const IntegrateArgs &a) { return a.noise; }
     __device__ static double *hist(const IntegrateArgs &a) { return a.hist; }
-    __device__ static const double *ell_w(const IntegrateArgs &a) { return a.ell_w; }
+    using Ell = int4;  // {weight lo, weight hi, ring-buffer offset, 0}
+    __device__ static const int4 *ell(const IntegrateArgs &a) { return a.ell_pk64; }
+    __device__ static double ell_w(const int4 v) { return __hiloint2double(v.y, v.x); }
+    __device__ static int ell_off(const int4 v) { return v.z; }
 };
 template <>
 struct SimArrays<float> {
     __device__ static const float *sc(const IntegrateArgs &a) { return a.sc_f32; }
     __device__ static const float *noise(const IntegrateArgs &a) { return a.noise_f32; }
     __device__ static float *hist(const IntegrateArgs &a) { return a.hist_f32; }
-    __device__ static const float *ell_w(const IntegrateArgs &a) { return a.ell_w32; }
+    using Ell = int2;  // {ring-buffer offset, weight bits}
+    __device__ static const int2 *ell(const IntegrateArgs &a) { return a.ell_pk32; }
+    __device__ static float ell_w(const int2 v) { return __int_as_float(v.y); }
+    __device__ static int ell_off(const int2 v) { return v.x; }
 };
 
 // FP32 coupling input of node j, sum_k SC[k][j] x[k] (x in shared memory, 16-byte
@@ -77,9 +83,13 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     const int sc_i = a.sc_idx[sim];
     const R *SC = SimArrays<R>::sc(a) + (size_t)sc_i * n * n;
     // sparse coupling: the nonzero sources of node j (ascending k), then zero-weight padding
+    using EA = SimArrays<R>;
     const int EK = SPARSE ? a.ell_k : 0;
-    const int *e_idx = SPARSE ? a.ell_idx + (size_t)sc_i * EK * n : nullptr;
-    const R *e_w = SPARSE ? SimArrays<R>::ell_w(a) + (size_t)sc_i * EK * n : nullptr;
+    const typename EA::Ell *pk = nullptr;
+    if (SPARSE && act) {
+        const int table = DELAY ? a.delay_idx[sim] : 0;
+        pk = EA::ell(a) + ((size_t)sc_i * a.ell_tables + table) * EK * n + j;
+    }
     const R *noise = SimArrays<R>::noise(a);
     R g[M::NG], iv[M::NI];
     P r[M::NR];
@@ -103,12 +113,10 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     int D = 0, buff = 0;
     S *hist = nullptr;
     const int *dly = nullptr;
-    const int *e_dly = nullptr;
     if (DELAY) {
         D = a.max_delay[sim];
         hist = SimArrays<S>::hist(a) + a.hist_off[sim];
         dly = a.delay + (size_t)a.delay_idx[sim] * n * n;
-        if (SPARSE) e_dly = a.ell_delay + ((size_t)sc_i * a.n_delay_tables + a.delay_idx[sim]) * EK * n;
         buff = D - 1;
     }
     auto reset_conn = [&]() {
@@ -129,23 +137,27 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
             R in = R(0);
             if (act) {
                 if (SPARSE && DELAY) {
-                    const S xj = hist[(size_t)buff * n + j];
+                    // ((buff + d) mod D) * n + k as buff * n + (d * n + k), wrapped once
+                    // (buff < D and d <= D); the host keeps 2 * D * n below 2^31.
+                    const int hbase = buff * n, hwrap = D * n;
+                    const S xj = hist[hbase + j];
+#pragma unroll 4
                     for (int q = 0; q < EK; ++q) {
-                        const size_t e = (size_t)q * n + j;
-                        const int k = __ldg(&e_idx[e]);
-                        int kb = buff + __ldg(&e_dly[e]);
-                        if (kb >= D) kb -= D;
-                        const S xk = hist[(size_t)kb * n + k];
-                        if (M::OSC) in += __ldg(&e_w[e]) * sin(R(xk - xj));
-                        else in += __ldg(&e_w[e]) * R(xk);
+                        const auto v = __ldg(pk + (size_t)q * n);
+                        int h = hbase + EA::ell_off(v);
+                        if (h >= hwrap) h -= hwrap;
+                        const S xk = hist[h];
+                        if (M::OSC) in += EA::ell_w(v) * sin(R(xk - xj));
+                        else in += EA::ell_w(v) * R(xk);
                     }
                 } else if (SPARSE) {
                     const S xj = x1[j];
+#pragma unroll 4
                     for (int q = 0; q < EK; ++q) {
-                        const size_t e = (size_t)q * n + j;
-                        const S xk = x1[__ldg(&e_idx[e])];
-                        if (M::OSC) in += __ldg(&e_w[e]) * sin(R(xk - xj));
-                        else in += __ldg(&e_w[e]) * R(xk);
+                        const auto v = __ldg(pk + (size_t)q * n);
+                        const S xk = x1[EA::ell_off(v)];
+                        if (M::OSC) in += EA::ell_w(v) * sin(R(xk - xj));
+                        else in += EA::ell_w(v) * R(xk);
                     }
                 } else if (DELAY) {
                     const S xj = hist[(size_t)buff * n + j];

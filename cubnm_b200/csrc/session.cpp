@@ -305,7 +305,7 @@ struct Session {
     // run buffers
     DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
-    DBuf d_tiles, d_sct_f32, d_ell_idx, d_ell_w, d_ell_w32, d_ell_delay;
+    DBuf d_tiles, d_sct_f32, d_ell_pk;
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -341,7 +341,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_idx, &S.d_ell_w, &S.d_ell_w32, &S.d_ell_delay,
+                        &S.d_sct_f32, &S.d_ell_pk,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -655,6 +655,8 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         // used when the densest column of every SC holds at most half the nodes
         // (CBNM_COUPLING=sparse|dense overrides).  Zero weights are skipped and the
         // nonzeros summed in ascending source order, so FP64 sums are unchanged.
+        // The packed ring-buffer offsets are 32-bit: every simulation's buffer must
+        // hold fewer than 2^30 values, else the dense loop runs.
         std::vector<double> sc_host;
         const double *src = h_sc;
         if (device_io) {
@@ -671,49 +673,53 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
             }
         const char *cpl = std::getenv("CBNM_COUPLING");
         const std::string mode = cpl ? cpl : "";
-        const bool sparse = mode == "sparse" || (mode != "dense" && n >= 32 && 2 * kmax <= n);
+        const long long max_hist = has_delay ? (long long)*std::max_element(h_max_delay.begin(), h_max_delay.end()) * n : 0;
+        const bool fits = max_hist < (1LL << 30);
+        const bool sparse = fits && (mode == "sparse" || (mode != "dense" && n >= 32 && 2 * kmax <= n));
         if (sparse) {
             const int K = std::max(kmax, 1);
-            const int n_tables = has_delay ? (int)(h_delay.size() / nn) : 0;
-            const size_t per_sc = (size_t)K * n;
-            std::vector<int> idx(per_sc * a->n_scs);
-            std::vector<double> w(per_sc * a->n_scs, 0.0);
-            std::vector<float> w32(per_sc * a->n_scs, 0.0f);
-            std::vector<int> edl(has_delay ? per_sc * a->n_scs * n_tables : 0, 1);
-            for (int sc = 0; sc < a->n_scs; ++sc)
-                for (int j = 0; j < n; ++j) {
-                    int q = 0;
-                    for (int k = 0; k < n; ++k) {
-                        const double v = src[(size_t)sc * nn + (size_t)k * n + j];
-                        if (v == 0.0) continue;
-                        const size_t e = (size_t)sc * per_sc + (size_t)q * n + j;
-                        idx[e] = k; w[e] = v; w32[e] = (float)v;
-                        for (int t = 0; t < n_tables; ++t)
-                            edl[((size_t)sc * n_tables + t) * per_sc + (size_t)q * n + j] =
-                                h_delay[(size_t)t * nn + (size_t)k * n + j];
-                        ++q;
-                    }
-                    for (; q < K; ++q) idx[(size_t)sc * per_sc + (size_t)q * n + j] = j;  // weight 0
+            const int tabs = has_delay ? (int)(h_delay.size() / nn) : 1;
+            const size_t per_tab = (size_t)K * n;
+            const size_t total = per_tab * tabs * a->n_scs;
+            std::vector<int2> pk32(c.fp32 ? total : 0);
+            std::vector<int4> pk64(c.fp32 ? 0 : total);
+            // padding: source j (delay 1 with delays), weight 0
+            auto put = [&](size_t e, int off, double v) {
+                if (c.fp32) {
+                    const float f = (float)v;
+                    int bits;
+                    std::memcpy(&bits, &f, sizeof(bits));
+                    pk32[e] = make_int2(off, bits);
+                } else {
+                    uint64_t u;
+                    std::memcpy(&u, &v, sizeof(u));
+                    pk64[e] = make_int4((int)(uint32_t)u, (int)(uint32_t)(u >> 32), off, 0);
                 }
-            S.d_ell_idx.ensure(sizeof(int) * idx.size());
-            CK(cudaMemcpyAsync(S.d_ell_idx.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, S.st));
-            if (c.fp32) {
-                S.d_ell_w32.ensure(sizeof(float) * w32.size());
-                CK(cudaMemcpyAsync(S.d_ell_w32.p, w32.data(), sizeof(float) * w32.size(), cudaMemcpyHostToDevice, S.st));
-                ia.ell_w32 = S.d_ell_w32.as<float>();
-            } else {
-                S.d_ell_w.ensure(sizeof(double) * w.size());
-                CK(cudaMemcpyAsync(S.d_ell_w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, S.st));
-                ia.ell_w = S.d_ell_w.as<double>();
-            }
-            if (has_delay) {
-                S.d_ell_delay.ensure(sizeof(int) * edl.size());
-                CK(cudaMemcpyAsync(S.d_ell_delay.p, edl.data(), sizeof(int) * edl.size(), cudaMemcpyHostToDevice, S.st));
-                ia.ell_delay = S.d_ell_delay.as<int>();
-            }
-            ia.ell_idx = S.d_ell_idx.as<int>();
+            };
+            for (int sc = 0; sc < a->n_scs; ++sc)
+                for (int t = 0; t < tabs; ++t) {
+                    const int *dl = has_delay ? h_delay.data() + (size_t)t * nn : nullptr;
+                    const size_t base = ((size_t)sc * tabs + t) * per_tab;
+                    for (int j = 0; j < n; ++j) {
+                        int q = 0;
+                        for (int k = 0; k < n; ++k) {
+                            const double v = src[(size_t)sc * nn + (size_t)k * n + j];
+                            if (v == 0.0) continue;
+                            const int d = dl ? dl[(size_t)k * n + j] : 0;
+                            put(base + (size_t)q * n + j, d * n + k, v);
+                            ++q;
+                        }
+                        for (; q < K; ++q) put(base + (size_t)q * n + j, (dl ? n : 0) + j, 0.0);
+                    }
+                }
+            const size_t bytes = c.fp32 ? sizeof(int2) * total : sizeof(int4) * total;
+            S.d_ell_pk.ensure(bytes);
+            CK(cudaMemcpyAsync(S.d_ell_pk.p, c.fp32 ? (const void *)pk32.data() : (const void *)pk64.data(), bytes,
+                               cudaMemcpyHostToDevice, S.st));
+            if (c.fp32) ia.ell_pk32 = S.d_ell_pk.as<int2>();
+            else ia.ell_pk64 = S.d_ell_pk.as<int4>();
             ia.ell_k = K;
-            ia.n_delay_tables = n_tables;
+            ia.ell_tables = tabs;
             CK(cudaStreamSynchronize(S.st));  // host vectors go out of scope
         }
     }

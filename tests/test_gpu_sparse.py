@@ -36,8 +36,8 @@ def _run(args, monkeypatch, mode):
     return core.run_simulations(*[x.copy() if isinstance(x, np.ndarray) else x for x in args])
 
 
-@pytest.mark.parametrize("model,delay", [("rWW", False), ("rWW", True), ("WC", True), ("JR", False),
-                                         ("rWWEx", True), ("Kuramoto", False)])
+@pytest.mark.parametrize("model,delay", [("rWW", False), ("rWW", True), ("WC", True), ("JR", False), ("JR", True),
+                                         ("rWWEx", True), ("Kuramoto", False), ("Kuramoto", True)])
 def test_fp64_sparse_equals_dense(model, delay, monkeypatch):
     args = _sparse_args(model, 8, 96, 8, 0.1, delay)
     dense, sparse = _run(args, monkeypatch, "dense"), _run(args, monkeypatch, "sparse")
