@@ -75,7 +75,7 @@ __device__ __forceinline__ Params load_params(const IntegrateArgs &a, int sim, i
 }
 
 // One integration step of node j (the coupling input already formed), exactly as
-// k_integrate_sim<RWWm<float>, false, float>.
+// k_integrate_sim<RWWm<float>, false, float, ...>.
 __device__ __forceinline__ void fwd_step(float *s, const Params &P, float in, const IntegrateArgs &a, int sh_ts,
                                          int inner, int sh_j) {
     const long long ni = ((long long)sh_ts * a.inner_it + inner) * a.nodes * M::NN + (long long)sh_j * M::NN;

@@ -68,8 +68,10 @@ __device__ __forceinline__ float coupling_f32(const float *__restrict__ SC, cons
     return (s0 + s1) + (s2 + s3);
 }
 
-template <class M, bool DELAY, class R, bool SPARSE>
-__global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
+// MAXT = the block size bound: 1024 (at most 64 registers a thread), or 512 (up
+// to 128 registers, no spills) for delayed networks of 129-512 nodes.
+template <class M, bool DELAY, class R, bool SPARSE, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_integrate_sim(const IntegrateArgs a) {
     const int sim = a.sim_begin + blockIdx.x;
     const int j = threadIdx.x;
     const int n = a.nodes;
@@ -281,29 +283,40 @@ __global__ void __launch_bounds__(1024) k_integrate_sim(const IntegrateArgs a) {
     }
 }
 
-template <class M, class R>
+template <class M, class R, int MAXT, bool DELAY>
+cudaError_t launch_sim_variant(const IntegrateArgs &a, int grid, int threads, size_t smem, cudaStream_t st) {
+    if (a.ell_k > 0) k_integrate_sim<M, DELAY, R, true, MAXT><<<grid, threads, smem, st>>>(a);
+    else k_integrate_sim<M, DELAY, R, false, MAXT><<<grid, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// UNCAP: with delays at 129-512 nodes, launch the 512-thread-bound variant.  Its
+// extra registers cost CTAs per SM; measured on one B200 (FP32 unless noted,
+// 8 s, 20% density, 6 m/s) it gains with delays: rWW 200 nodes FP64 1.59x, rWW
+// 400 1.40x, rWW 512 1.47x, WC 300 1.50x, JR 160 1.64x, rWW 400 FP64 1.01x; but
+// rWWEx 200 0.85x (its capped variant does not spill), and without delays
+// 0.77-0.88x (rWW 200 and 256 nodes, FP32 and FP64), so those keep the cap
+// (as does Kuramoto, not measured).
+template <class M, class R, bool UNCAP>
 cudaError_t launch_sim_kernel(const IntegrateArgs &a, cudaStream_t st) {
     const int threads = ((a.nodes + 31) / 32) * 32;
     const size_t smem = a.has_delay ? 0 : sizeof(typename M::S) * a.nodes;
     const int grid = a.n_sims - a.sim_begin;
-    if (a.ell_k > 0) {
-        if (a.has_delay) k_integrate_sim<M, true, R, true><<<grid, threads, smem, st>>>(a);
-        else k_integrate_sim<M, false, R, true><<<grid, threads, smem, st>>>(a);
-    } else {
-        if (a.has_delay) k_integrate_sim<M, true, R, false><<<grid, threads, smem, st>>>(a);
-        else k_integrate_sim<M, false, R, false><<<grid, threads, smem, st>>>(a);
+    if (!a.has_delay) return launch_sim_variant<M, R, 1024, false>(a, grid, threads, smem, st);
+    if constexpr (UNCAP) {
+        if (threads > 128 && threads <= 512) return launch_sim_variant<M, R, 512, true>(a, grid, threads, smem, st);
     }
-    return cudaGetLastError();
+    return launch_sim_variant<M, R, 1024, true>(a, grid, threads, smem, st);
 }
 
 template <class R>
 cudaError_t launch_sim_model(int model, const IntegrateArgs &a, cudaStream_t st) {
     switch (model) {
-        case MODEL_RWW: return launch_sim_kernel<RWWm<R>, R>(a, st);
-        case MODEL_WC: return launch_sim_kernel<WCm<R>, R>(a, st);
-        case MODEL_JR: return launch_sim_kernel<JRm<R>, R>(a, st);
-        case MODEL_KURAMOTO: return launch_sim_kernel<Kuramotom<R>, R>(a, st);
-        case MODEL_RWWEX: return launch_sim_kernel<RWWExm<R>, R>(a, st);
+        case MODEL_RWW: return launch_sim_kernel<RWWm<R>, R, true>(a, st);
+        case MODEL_WC: return launch_sim_kernel<WCm<R>, R, true>(a, st);
+        case MODEL_JR: return launch_sim_kernel<JRm<R>, R, true>(a, st);
+        case MODEL_KURAMOTO: return launch_sim_kernel<Kuramotom<R>, R, false>(a, st);  // not measured
+        case MODEL_RWWEX: return launch_sim_kernel<RWWExm<R>, R, false>(a, st);
     }
     return cudaErrorInvalidValue;
 }
