@@ -52,7 +52,7 @@ class SimGroup:
         self.noise_out = noise_out
         self.gof_terms = list(gof_terms)
         self.do_fc = do_fc
-        self.do_fcd = do_fcd and do_fc
+        self.do_fcd = do_fcd
         self.window_size = window_size
         self.window_step = window_step
         self.window_size_TRs = int(np.round(window_size / (TR * 2))) * 2  # base.py:468-476
@@ -82,6 +82,36 @@ class SimGroup:
         self._N = 0
 
     # -- properties mirrored from base.py
+    @property
+    def do_fc(self):
+        return self._do_fc
+
+    @do_fc.setter
+    def do_fc(self, do_fc):  # base.py:486-496
+        if hasattr(self, "gof_terms") and not do_fc and \
+                any(t in self.gof_terms for t in ("+fc_corr", "-fc_diff", "-fc_normec")):
+            raise ValueError("Cannot calculate FC goodness-of-fit terms without FC."
+                             " Set do_fc to True or remove FC-related goodness-of-fit terms.")
+        if getattr(self, "_do_fcd", False) and not do_fc:
+            raise ValueError("Cannot calculate FCD without FC. Set do_fcd to False.")
+        self._do_fc = do_fc
+
+    @property
+    def do_fcd(self):
+        return self._do_fcd
+
+    @do_fcd.setter
+    def do_fcd(self, do_fcd):  # base.py:502-513
+        if getattr(self, "_do_fc", False):
+            self._do_fcd = do_fcd
+        elif do_fcd:
+            raise ValueError("Cannot calculate FCD without FC")
+        else:
+            self._do_fcd = False
+        if hasattr(self, "gof_terms") and not self._do_fcd and "-fcd_ks" in self.gof_terms:
+            raise ValueError("Cannot calculate FCD goodness-of-fit terms without FCD."
+                             " Set do_fcd to True or remove FCD-related goodness-of-fit terms.")
+
     @property
     def N(self):
         return self._N

@@ -1,0 +1,219 @@
+"""Records the arguments the reference's ``SimGroup.run()`` hands to its compiled
+core, for the CPU test of ``cubnm_b200.sim`` (``tests/test_sim_marshalling.py``).
+
+Run once, in a checkout that has the reference next to it:
+
+    python tests/golden/make_simgroup_args.py /path/to/cubnm
+
+It imports the reference's Python package (``src/cubnm``) with its compiled
+extension replaced by a recorder: ``cubnm._core.run_simulations`` stores its 22
+positional arguments (``src/cubnm/sim/base.py:727-750``) and stops the run, and
+``cubnm._setup_opts`` (written by the reference's build) is given the flags of a
+regular NVIDIA GPU build (no many-nodes mode); every group is made with
+``force_gpu=True``.  Nothing is simulated.
+
+Each case of ``CASES`` and ``MULTI`` below is built through
+``build(simmod, case)`` for any module with the reference's SimGroup classes, so
+the test builds the same groups with ``cubnm_b200.sim``.
+
+The cases of ``SCORE_CASES`` are run once more with the recorder answering
+``fake_outputs()`` (no simulation: seeded arrays of the output shapes), then
+scored by the reference's ``score()`` against ``empirical()``; with no CuPy the
+reference computes every term on the CPU with scipy (``base.py:1163-1188``).
+
+Output: ``tests/golden/simgroup_args.npz`` with, per case, the array arguments
+as ``<case>|<index>``, the rest as JSON in ``<case>|meta``, and for the scored
+groups ``<case>|<child>|score|<column>`` plus the processed rWW FIC outputs.
+"""
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "simgroup_args.npz")
+NODES = 10
+ARRAY_ARGS = (1, 2, 3, 4, 5, 6)  # sc, sc_indices, sc_dist, global, regional, v
+
+
+def _sc(seed, nodes=NODES):
+    rng = np.random.default_rng(seed)
+    w = np.triu(rng.lognormal(0.0, 1.0, (nodes, nodes)) * (rng.random((nodes, nodes)) < 0.4), 1)
+    w = w + w.T
+    return w / w.sum(axis=1).mean()
+
+
+def _dist(seed, nodes=NODES):
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(-50, 50, (nodes, 3))
+    return np.linalg.norm(pts[:, None] - pts[None], axis=2) * 1.3
+
+
+# name: (class, constructor kwargs, N, parameters, extra attributes)
+CASES = {
+    "rww_fic": ("rWWSimGroup", dict(duration=60, TR=1, window_size=10, window_step=2), 3,
+                {"G": [0.5, 1.0, 2.0]}, {}),
+    "rww_delay": ("rWWSimGroup", dict(duration=20, TR=0.5, dt="0.1", bw_dt="0.5", states_ts=True, noise_out=True,
+                                      do_fic=False, bold_remove_s=2, window_size=5, window_step=1, sim_seed=7,
+                                      noise_segment_length=10, gof_terms=["+fc_corr", "-fc_diff", "-fcd_ks"],
+                                      sc_dist="dist"), 4,
+                  {"G": [0.1, 0.2, 0.3, 0.4], "w_p": "per_node", "v": [1.0, 2.0, 3.0, 4.0]}, {}),
+    "rww_numfic": ("rWWSimGroup", dict(duration=30, TR=1, do_fic=True, max_fic_trials=5, fcd_drop_edges=False,
+                                       exc_interhemispheric=False), 2, {"G": [0.3, 0.6], "J_N": [0.12, 0.2]}, {}),
+    "wc": ("WCSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2), 2,
+           {"G": [0.5, 1.5]}, {}),
+    "jr": ("JRSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2, do_fcd=False,
+                                   gof_terms=["+fc_corr"]), 2,
+           {"G": [1.0, 2.0]}, {}),
+    "kuramoto": ("KuramotoSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
+                                          sim_seed=3), 2, {"G": [0.2, 0.4]}, {}),
+    "rwwex": ("rWWExSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
+                                    do_fc=False, do_fcd=False, gof_terms=[]), 2, {"G": [0.2, 0.4]}, {}),
+    "rww_child": ("rWWSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
+                                      do_fic=False), 2, {"G": [0.2, 0.4]}, {}),
+}
+
+# groups of children run as one (MultiSimGroupMixin): (case, SC seed, N) per child;
+# the third child repeats the first one's SC
+MULTI = {
+    "rww_multi": ("rWWSimGroup", [("rww_child", 1, 2), ("rww_child", 2, 3), ("rww_child", 1, 1)]),
+}
+
+
+def build(simmod, name, sc_seed=1, N=None):
+    """The SimGroup of case `name` (of ``CASES`` or ``MULTI``), from the classes
+    of module `simmod`, with N and its parameters set and the defaults filled in."""
+    if name in MULTI:
+        cls, children = MULTI[name]
+        kids = [build(simmod, c, seed, n) for c, seed, n in children]
+        return simmod.create_multi_sim_group(getattr(simmod, cls))(kids)
+    cls, kw, n_default, params, extra = CASES[name]
+    N = n_default if N is None else N
+    kw = dict(kw, force_gpu=True)  # the GPU path, whether or not this host has a GPU
+    kw["sc"] = _sc(sc_seed)
+    if kw.get("sc_dist") == "dist":
+        kw["sc_dist"] = _dist(5)
+    sg = getattr(simmod, cls)(**kw)
+    sg.N = N
+    rng = np.random.default_rng(11 + sc_seed)
+    for p, v in params.items():
+        if isinstance(v, str):
+            sg.param_lists[p] = rng.uniform(0.5, 1.5, (N, sg.nodes))
+        else:
+            v = np.resize(np.asarray(v, dtype=float), N)
+            if p in sg.regional_param_names:
+                v = np.repeat(v[:, None], sg.nodes, axis=1)
+            sg.param_lists[p] = v
+    for k, v in extra.items():
+        setattr(sg, k, np.asarray(v))
+    sg._set_default_params()
+    return sg
+
+
+# cases whose run() is answered by fake_outputs() and then scored
+SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi")
+N_EMP_FCD = 12
+
+
+def fake_outputs(args, n_state):
+    """A deterministic stand-in for run_simulations' output dict (the keys and
+    shapes of ``src/ext/core.cpp:453-492``), seeded from N and nodes: FC rows
+    (row 1 all NaN), FCD rows, time-averaged states with the rWW r_E state
+    spread over 1-5 Hz (so the FIC penalty sees both branches), FIC flags."""
+    N, nodes, cfg = args[14], args[15], args[7]
+    rng = np.random.default_rng(1000 + 31 * N + nodes)
+    bold_len = args[16] // args[17]
+    out = {"init_time": 0.0, "run_time": 0.0,
+           "sim_bold": rng.normal(size=(N, bold_len * nodes)),
+           "_sim_states": rng.uniform(1.0, 5.0, (n_state, N, nodes)),
+           "_global_bools": (rng.random((2, N)) < 0.5),
+           "_global_ints": rng.integers(0, 5, (1, N)).astype(np.intc)}
+    if cfg["do_fc"] == "1":
+        fc = rng.uniform(-1, 1, (N, nodes * (nodes - 1) // 2))
+        if N > 1:
+            fc[1] = np.nan
+        out["sim_fc_trils"] = fc
+        if cfg["do_fcd"] == "1":
+            out["sim_fcd_trils"] = rng.uniform(-1, 1, (N, 10))
+    return out
+
+
+def empirical(nodes):
+    rng = np.random.default_rng(77)
+    return rng.uniform(-1, 1, nodes * (nodes - 1) // 2), rng.uniform(-1, 1, N_EMP_FCD)
+
+
+def _reference_sim(ref_root):
+    """Imports src/cubnm/sim from the reference with a recording core."""
+    class Stop(Exception):
+        pass
+
+    rec = {}
+
+    def run_simulations(*args):
+        rec["args"] = args
+        if rec.get("answer"):
+            return fake_outputs(args, rec["n_state"])
+        raise Stop()
+
+    def stub(name, **attrs):
+        m = types.ModuleType(name)
+        m.__dict__.update(attrs)
+        sys.modules[name] = m
+        return m
+
+    pkg = stub("cubnm")
+    pkg.__path__ = [os.path.join(ref_root, "src", "cubnm")]
+    pkg._core = stub("cubnm._core", run_simulations=run_simulations, set_const=lambda *a: None, init=lambda: None)
+    pkg._setup_opts = stub("cubnm._setup_opts", many_nodes_flag=False, gpu_enabled_flag=True, max_nodes_reg=200,
+                           max_nodes_many=500, noise_segment_flag=True, gpu_model_flag="nvidia")
+    pkg._version = stub("cubnm._version", get_versions=lambda: {"version": "0+recorded"})
+    import cubnm.sim as refsim
+    return refsim, rec, Stop
+
+
+def main(ref_root):
+    refsim, rec, Stop = _reference_sim(ref_root)
+    out = {}
+    for name in list(CASES) + list(MULTI):
+        sg = build(refsim, name)
+        rec.clear()
+        try:
+            sg.run()
+        except Stop:
+            pass
+        args = rec["args"]
+        assert len(args) == 22, len(args)
+        for i in ARRAY_ARGS:
+            out[f"{name}|{i}"] = np.asarray(args[i])
+        meta = {str(i): args[i] for i in range(22) if i not in ARRAY_ARGS and i != 7}
+        meta["model_config"] = args[7]
+        out[f"{name}|meta"] = np.array(json.dumps(meta, sort_keys=True))
+    if not hasattr(np, "NaN"):  # the reference's rww.py:220 predates numpy 2
+        np.NaN = np.nan
+    for name in SCORE_CASES:
+        sg = build(refsim, name)
+        rec.clear()
+        rec["answer"] = True
+        rec["n_state"] = len(sg.state_names) if hasattr(sg, "state_names") else None
+        sg.run()
+        emp_fc, emp_fcd = empirical(sg.nodes)
+        for g, grp in enumerate(getattr(sg, "children", [sg])):
+            key = f"{name}|{g}"
+            scores = grp.score(emp_fc, emp_fcd)
+            out[f"{key}|score_columns"] = np.array(json.dumps(sorted(scores.columns)))
+            for c in scores.columns:
+                out[f"{key}|score|{c}"] = scores[c].to_numpy(dtype=float)
+            out[f"{key}|bold_shape"] = np.asarray(grp.sim_bold.shape)
+            if getattr(grp, "do_fic", False):
+                out[f"{key}|wIE"] = np.asarray(grp.param_lists["wIE"], dtype=float)
+                out[f"{key}|fic_ntrials"] = np.asarray(grp.fic_ntrials)
+                out[f"{key}|fic_failed"] = np.asarray(grp.fic_failed)
+    np.savez_compressed(OUT, **out)
+    print(f"wrote {OUT}: {len(CASES) + len(MULTI)} cases")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUBNM_REFERENCE", "../cubnm"))

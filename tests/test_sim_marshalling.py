@@ -1,0 +1,115 @@
+"""SimGroup marshalling against the reference's own SimGroup (CPU).
+
+``tests/golden/simgroup_args.npz`` holds the 22 arguments that the reference's
+``SimGroup.run()`` (``src/cubnm/sim/base.py:673-752``) and
+``MultiSimGroupMixin.run()`` (``base.py:1323-1385``) pass to
+``run_simulations`` for the groups of ``tests/golden/make_simgroup_args.py``.
+Here the same groups are built with ``cubnm_b200.sim`` and run with
+``core.run_simulations`` replaced by a recorder: every argument must be equal,
+and ``model_config`` may differ only by the ``precision`` key this library adds.
+The checks of ``do_fc`` / ``do_fcd`` / ``gof_terms`` follow ``base.py:486-513``.
+
+The fixture also holds the reference's ``score()`` of groups whose run was
+answered by ``fake_outputs()``; the same outputs go through this library's
+``_process_out`` / ``score`` with the GPU goodness-of-fit call replaced by the
+reference's CPU formulas (``base.py:1164-1188``), so what is compared is the
+output handling, signs, NaN fill, ``+gof`` and the rWW FIC penalty.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+import scipy.stats
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_simgroup_args as G  # noqa: E402
+from cubnm_b200 import sim  # noqa: E402
+
+FIXTURE = np.load(os.path.join(os.path.dirname(__file__), "golden", "simgroup_args.npz"))
+
+
+class _Stop(Exception):
+    pass
+
+
+def _recorded_args(sg, monkeypatch):
+    rec = {}
+
+    def run_simulations(*args):
+        rec["args"] = args
+        raise _Stop()
+
+    monkeypatch.setattr(sim.core, "run_simulations", run_simulations)
+    with pytest.raises(_Stop):
+        sg.run()
+    return rec["args"]
+
+
+@pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI))
+def test_run_arguments_equal_the_reference(case, monkeypatch):
+    args = _recorded_args(G.build(sim, case), monkeypatch)
+    assert len(args) == 22
+    for i in G.ARRAY_ARGS:
+        ref = FIXTURE[f"{case}|{i}"]
+        got = np.asarray(args[i])
+        assert got.shape == ref.shape, (i, got.shape, ref.shape)
+        np.testing.assert_array_equal(got, ref, err_msg=f"argument {i}")
+    meta = json.loads(str(FIXTURE[f"{case}|meta"]))
+    ref_cfg = meta.pop("model_config")
+    for k, v in meta.items():
+        assert args[int(k)] == v, (k, args[int(k)], v)
+    cfg = dict(args[7])
+    assert cfg.pop("precision") == "fp64"
+    assert cfg == ref_cfg
+
+
+def test_fc_fcd_and_gof_term_checks():
+    sc = G._sc(1)
+    with pytest.raises(ValueError, match="FCD without FC"):
+        sim.rWWSimGroup(duration=10, TR=1, sc=sc, do_fc=False, gof_terms=[])
+    with pytest.raises(ValueError, match="FC goodness-of-fit terms without FC"):
+        sim.rWWSimGroup(duration=10, TR=1, sc=sc, do_fc=False, do_fcd=False)
+    with pytest.raises(ValueError, match="FCD goodness-of-fit terms without FCD"):
+        sim.rWWSimGroup(duration=10, TR=1, sc=sc, do_fcd=False)
+    sg = sim.rWWSimGroup(duration=10, TR=1, sc=sc, do_fc=False, do_fcd=False, gof_terms=[])
+    assert not sg.do_fc and not sg.do_fcd
+
+
+def _cpu_gof(sim_fc_trils=None, emp_fc_tril=None, sim_fcd_trils=None, emp_fcd_tril=None, terms=None):
+    """The reference's CPU goodness-of-fit formulas (base.py:1164-1188), as
+    positive distances / correlations like ``utils.gof``."""
+    out = {}
+    if sim_fc_trils is not None:
+        if "fc_corr" in terms:
+            out["fc_corr"] = np.array([scipy.stats.pearsonr(r, emp_fc_tril).statistic for r in sim_fc_trils])
+        if "fc_diff" in terms:
+            out["fc_diff"] = np.abs(sim_fc_trils.mean(axis=1) - emp_fc_tril.mean())
+        if "fc_normec" in terms:
+            out["fc_normec"] = np.linalg.norm(sim_fc_trils - emp_fc_tril[None], axis=1) / (2 * np.sqrt(emp_fc_tril.size))
+    if sim_fcd_trils is not None and "fcd_ks" in terms:
+        out["fcd_ks"] = np.array([scipy.stats.ks_2samp(r, emp_fcd_tril).statistic for r in sim_fcd_trils])
+    return out
+
+
+@pytest.mark.parametrize("case", G.SCORE_CASES)
+def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
+    sg = G.build(sim, case)
+    monkeypatch.setattr(sim.core, "run_simulations", lambda *a: G.fake_outputs(a, len(sg.state_names)))
+    monkeypatch.setattr(sim.utils, "gof", _cpu_gof)
+    sg.run()
+    emp_fc, emp_fcd = G.empirical(sg.nodes)
+    for g, grp in enumerate(getattr(sg, "children", [sg])):
+        key = f"{case}|{g}"
+        with np.errstate(invalid="ignore"):
+            scores = grp.score(emp_fc, emp_fcd)
+        assert sorted(scores.columns) == json.loads(str(FIXTURE[f"{key}|score_columns"]))
+        for c in scores.columns:
+            np.testing.assert_allclose(scores[c].to_numpy(dtype=float), FIXTURE[f"{key}|score|{c}"],
+                                       rtol=1e-12, atol=1e-15, err_msg=c)
+        assert tuple(grp.sim_bold.shape) == tuple(FIXTURE[f"{key}|bold_shape"])
+        if getattr(grp, "do_fic", False):
+            np.testing.assert_array_equal(grp.param_lists["wIE"], FIXTURE[f"{key}|wIE"])
+            np.testing.assert_array_equal(grp.fic_ntrials, FIXTURE[f"{key}|fic_ntrials"])
+            np.testing.assert_array_equal(grp.fic_failed, FIXTURE[f"{key}|fic_failed"])
