@@ -21,6 +21,11 @@ The cases of ``SCORE_CASES`` are run once more with the recorder answering
 scored by the reference's ``score()`` against ``empirical()``; with no CuPy the
 reference computes every term on the CPU with scipy (``base.py:1163-1188``).
 
+``UTIL_CASES`` records the reference's empirical helpers
+(``src/cubnm/utils.py:130-304``: ``get_bw_params``, ``calculate_fc``,
+``calculate_fcd``) on seeded BOLD arrays with zeroed (outlier) volumes,
+inter-hemispheric exclusion, edge windows kept and windows dropped as outliers.
+
 Output: ``tests/golden/simgroup_args.npz`` with, per case, the array arguments
 as ``<case>|<index>``, the rest as JSON in ``<case>|meta``, and for the scored
 groups ``<case>|<child>|score|<column>`` plus the processed rWW FIC outputs.
@@ -145,6 +150,23 @@ def empirical(nodes):
     return rng.uniform(-1, 1, nodes * (nodes - 1) // 2), rng.uniform(-1, 1, N_EMP_FCD)
 
 
+# empirical-helper cases: (BOLD seed, zeroed volumes, FC kwargs, FCD args and kwargs)
+UTIL_CASES = {
+    "plain": (21, [], {}, (10, 2), {}),
+    "outliers_hemi": (22, [5, 6, 40], {"exc_interhemispheric": True}, (8, 2),
+                      {"exc_interhemispheric": True, "return_dfc": True}),
+    "no_drop_edges": (23, [], {}, (6, 3), {"drop_edges": False}),
+    "outlier_windows": (24, list(range(10, 19)), {}, (6, 2), {"outlier_threshold": 0.5}),
+}
+
+
+def util_bold(seed, zeroed, nodes=NODES, vols=60):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(nodes, vols)).cumsum(axis=1)
+    x[:, zeroed] = 0.0
+    return x
+
+
 def _reference_sim(ref_root):
     """Imports src/cubnm/sim from the reference with a recording core."""
     class Stop(Exception):
@@ -211,6 +233,18 @@ def main(ref_root):
                 out[f"{key}|wIE"] = np.asarray(grp.param_lists["wIE"], dtype=float)
                 out[f"{key}|fic_ntrials"] = np.asarray(grp.fic_ntrials)
                 out[f"{key}|fic_failed"] = np.asarray(grp.fic_failed)
+    import cubnm.utils as refutils
+    for name, (seed, zeroed, fc_kw, fcd_args, fcd_kw) in UTIL_CASES.items():
+        bold = util_bold(seed, zeroed)
+        out[f"util|{name}|fc"] = refutils.calculate_fc(bold.copy(), **fc_kw)
+        fcd = refutils.calculate_fcd(bold.copy(), *fcd_args, **fcd_kw)
+        if fcd_kw.get("return_dfc"):
+            out[f"util|{name}|fcd"], out[f"util|{name}|dfc"] = fcd
+        else:
+            out[f"util|{name}|fcd"] = fcd
+    for src in ("friston2003", "heinzle2016-3T"):
+        p = refutils.get_bw_params(src)
+        out[f"util|bw|{src}"] = np.array([p["k1"], p["k2"], p["k3"]])
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT}: {len(CASES) + len(MULTI)} cases")
 

@@ -113,3 +113,23 @@ def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
             np.testing.assert_array_equal(grp.param_lists["wIE"], FIXTURE[f"{key}|wIE"])
             np.testing.assert_array_equal(grp.fic_ntrials, FIXTURE[f"{key}|fic_ntrials"])
             np.testing.assert_array_equal(grp.fic_failed, FIXTURE[f"{key}|fic_failed"])
+
+
+@pytest.mark.parametrize("case", list(G.UTIL_CASES))
+def test_empirical_fc_fcd_equal_the_reference(case):
+    from cubnm_b200 import utils
+    seed, zeroed, fc_kw, fcd_args, fcd_kw = G.UTIL_CASES[case]
+    bold = G.util_bold(seed, zeroed)
+    np.testing.assert_allclose(utils.calculate_fc(bold, **fc_kw), FIXTURE[f"util|{case}|fc"], rtol=1e-12, atol=1e-14)
+    fcd = utils.calculate_fcd(bold, *fcd_args, **fcd_kw)
+    if fcd_kw.get("return_dfc"):
+        fcd, dfc = fcd
+        np.testing.assert_allclose(dfc, FIXTURE[f"util|{case}|dfc"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(fcd, FIXTURE[f"util|{case}|fcd"], rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("src", ["friston2003", "heinzle2016-3T"])
+def test_bw_params_equal_the_reference(src):
+    from cubnm_b200 import utils
+    p = utils.get_bw_params(src)
+    np.testing.assert_array_equal([p["k1"], p["k2"], p["k3"]], FIXTURE[f"util|bw|{src}"])
