@@ -30,6 +30,7 @@ Output: ``tests/golden/simgroup_args.npz`` with, per case, the array arguments
 as ``<case>|<index>``, the rest as JSON in ``<case>|meta``, and for the scored
 groups ``<case>|<child>|score|<column>`` plus the processed rWW FIC outputs.
 """
+import hashlib
 import json
 import os
 import sys
@@ -122,11 +123,12 @@ SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi")
 N_EMP_FCD = 12
 
 
-def fake_outputs(args, n_state):
+def fake_outputs(args, n_state, n_noise=1):
     """A deterministic stand-in for run_simulations' output dict (the keys and
     shapes of ``src/ext/core.cpp:453-492``), seeded from N and nodes: FC rows
     (row 1 all NaN), FCD rows, time-averaged states with the rWW r_E state
-    spread over 1-5 Hz (so the FIC penalty sees both branches), FIC flags."""
+    spread over 1-5 Hz (so the FIC penalty sees both branches), FIC flags, and
+    with ``noise_out`` a noise segment with node / time shuffles."""
     N, nodes, cfg = args[14], args[15], args[7]
     rng = np.random.default_rng(1000 + 31 * N + nodes)
     bold_len = args[16] // args[17]
@@ -135,6 +137,14 @@ def fake_outputs(args, n_state):
            "_sim_states": rng.uniform(1.0, 5.0, (n_state, N, nodes)),
            "_global_bools": (rng.random((2, N)) < 0.5),
            "_global_ints": rng.integers(0, 5, (1, N)).astype(np.intc)}
+    if args[10]:  # noise_out
+        bw_dt = args[21]
+        seg = int(int(cfg["noise_time_steps"]) / bw_dt)
+        inner = int(round(bw_dt / args[20]))
+        reps = -(-int(args[16] / bw_dt) // seg)
+        out["_noise"] = rng.normal(size=seg * inner * nodes * n_noise)
+        out["_shuffled_nodes"] = np.stack([rng.permutation(nodes) for _ in range(reps)]).astype(np.intc)
+        out["_shuffled_ts"] = np.stack([rng.permutation(seg) for _ in range(reps)]).astype(np.intc)
     if cfg["do_fc"] == "1":
         fc = rng.uniform(-1, 1, (N, nodes * (nodes - 1) // 2))
         if N > 1:
@@ -177,7 +187,7 @@ def _reference_sim(ref_root):
     def run_simulations(*args):
         rec["args"] = args
         if rec.get("answer"):
-            return fake_outputs(args, rec["n_state"])
+            return fake_outputs(args, rec["n_state"], rec["n_noise"])
         raise Stop()
 
     def stub(name, **attrs):
@@ -219,8 +229,12 @@ def main(ref_root):
         sg = build(refsim, name)
         rec.clear()
         rec["answer"] = True
-        rec["n_state"] = len(sg.state_names) if hasattr(sg, "state_names") else None
+        rec["n_state"], rec["n_noise"] = len(sg.state_names), sg.n_noise
         sg.run()
+        if sg.noise_out:
+            noise = np.ascontiguousarray(sg.get_noise())
+            out[f"{name}|noise_shape"] = np.asarray(noise.shape)
+            out[f"{name}|noise_sha256"] = np.array(hashlib.sha256(noise.tobytes()).hexdigest())
         emp_fc, emp_fcd = empirical(sg.nodes)
         for g, grp in enumerate(getattr(sg, "children", [sg])):
             key = f"{name}|{g}"

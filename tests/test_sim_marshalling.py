@@ -13,8 +13,10 @@ The fixture also holds the reference's ``score()`` of groups whose run was
 answered by ``fake_outputs()``; the same outputs go through this library's
 ``_process_out`` / ``score`` with the GPU goodness-of-fit call replaced by the
 reference's CPU formulas (``base.py:1164-1188``), so what is compared is the
-output handling, signs, NaN fill, ``+gof`` and the rWW FIC penalty.
+output handling, signs, NaN fill, ``+gof``, the rWW FIC penalty and the noise
+reconstruction of ``get_noise``.
 """
+import hashlib
 import json
 import os
 import sys
@@ -96,9 +98,13 @@ def _cpu_gof(sim_fc_trils=None, emp_fc_tril=None, sim_fcd_trils=None, emp_fcd_tr
 @pytest.mark.parametrize("case", G.SCORE_CASES)
 def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
     sg = G.build(sim, case)
-    monkeypatch.setattr(sim.core, "run_simulations", lambda *a: G.fake_outputs(a, len(sg.state_names)))
+    monkeypatch.setattr(sim.core, "run_simulations", lambda *a: G.fake_outputs(a, len(sg.state_names), sg.n_noise))
     monkeypatch.setattr(sim.utils, "gof", _cpu_gof)
     sg.run()
+    if sg.noise_out:  # get_noise, base.py:843-895
+        noise = np.ascontiguousarray(sg.get_noise())
+        assert noise.shape == tuple(FIXTURE[f"{case}|noise_shape"])
+        assert hashlib.sha256(noise.tobytes()).hexdigest() == str(FIXTURE[f"{case}|noise_sha256"])
     emp_fc, emp_fcd = G.empirical(sg.nodes)
     for g, grp in enumerate(getattr(sg, "children", [sg])):
         key = f"{case}|{g}"
