@@ -3,10 +3,14 @@
 Restates the parts of src/cubnm/sim/base.py that sit on the simulation path
 (``SimGroup.__init__`` settings, ``run`` base.py:673-766, ``_process_out``
 :768-818, ``get_noise`` :843-895, ``score`` :1084-1207,
-``MultiSimGroupMixin`` :1303-1438) and the per-model parameter surface of
-src/cubnm/sim/{rww,wc,jr,kuramoto,rwwex}.py.  Simulations run through
-``cubnm_b200.core.run_simulations``; the goodness-of-fit terms through the
-library's GPU kernels.  Plotting / saving helpers are not part of this path.
+``MultiSimGroupMixin`` :1303-1438), the hooks and result helpers that
+``cubnm.optimize.BNMProblem`` and the optimisers call (``_problem_init`` /
+``_problem_evaluate`` :1055-1082, ``get_state_averages``, ``get_sim_fc`` /
+``get_sim_fcd``, ``slice``, ``clear`` :820-1053) and the per-model parameter
+surface of src/cubnm/sim/{rww,wc,jr,kuramoto,rwwex}.py.  Simulations run
+through ``cubnm_b200.core.run_simulations``; the goodness-of-fit terms through
+the library's GPU kernels.  Plotting / saving helpers (``save``, ``labels``)
+are not part of this path.
 """
 import copy
 from decimal import Decimal
@@ -76,10 +80,15 @@ class SimGroup:
         for k in ("k1", "k2", "k3"):
             core.set_const(k, p[k])
         self.param_lists = {k: None for k in self.global_param_names + self.regional_param_names + ["v"]}
+        self.out_dir = out_dir  # where the reference's save() writes; saving is not part of this library
         self.last_N = 0
         self.last_config = self.get_config()
         self.it = 0
         self._N = 0
+        self.post_init()
+
+    def post_init(self):  # base.py:288-294
+        """Hook run at the end of __init__ (nothing by default)."""
 
     # -- properties mirrored from base.py
     @property
@@ -231,6 +240,87 @@ class SimGroup:
         parts = [seg[self._shuffled_ts[r]][:, :, self._shuffled_nodes[r]] for r in range(self._shuffled_nodes.shape[0])]
         return np.concatenate(parts, axis=0)[: self.bw_it].transpose(3, 2, 0, 1)
 
+    def get_state_averages(self):  # base.py:820-841
+        """Per-simulation averages of each state variable over time and nodes."""
+        avg = {}
+        for name in self.state_names:
+            v = self.sim_states[name]
+            avg[name] = v[:, self.n_states_samples_remove:, :].mean(axis=1).mean(axis=1) if self.states_ts \
+                else v.mean(axis=1)
+        return pd.DataFrame(avg)
+
+    def get_sim_fc(self, idx):  # base.py:897-942
+        """FC of simulation `idx` as a (nodes, nodes) matrix, diagonal 1 (NaN
+        between hemispheres when they are excluded)."""
+        if not self.do_fc:
+            raise ValueError("FC is not calculated in this simulation group")
+        if idx >= self.N:
+            raise IndexError("Index out of range")
+        tril = self.sim_fc_trils[idx]
+        fc = np.zeros((self.nodes, self.nodes))
+        if self.exc_interhemispheric:
+            h = self.nodes // 2
+            fc[:h, :h][np.tril_indices(h, -1)] = tril[: tril.shape[0] // 2]
+            fc[h:, h:][np.tril_indices(h, -1)] = tril[tril.shape[0] // 2:]
+            fc[:h, h:] = np.nan
+            fc[h:, :h] = np.nan
+        else:
+            fc[np.tril_indices(self.nodes, -1)] = tril
+        fc += fc.T
+        np.fill_diagonal(fc, 1.0)
+        return fc
+
+    def get_sim_fcd(self, idx):  # base.py:944-987
+        """FCD of simulation `idx` as a (windows, windows) matrix, diagonal 1."""
+        if not self.do_fcd:
+            raise ValueError("FCD is not calculated in this simulation group")
+        if idx >= self.N:
+            raise IndexError("Index out of range")
+        tril = self.sim_fcd_trils[idx]
+        w = (1 + np.sqrt(1 + 8 * tril.shape[0])) / 2  # windows from the pair count
+        assert w.is_integer()
+        w = int(w)
+        fcd = np.zeros((w, w))
+        fcd[np.tril_indices(w, -1)] = tril
+        fcd += fcd.T
+        np.fill_diagonal(fcd, 1.0)
+        return fcd
+
+    def slice(self, key, inplace=False):  # base.py:989-1028
+        """The group reduced to simulation `key` (a shallow copy unless `inplace`)."""
+        if not isinstance(key, int):
+            raise ValueError("Only integer indexing is supported")
+        if key >= self.N:
+            raise IndexError("Index out of range")
+        obj = self if inplace else copy.copy(self)
+        obj.param_lists = {k: v[key][np.newaxis, ...] for k, v in self.param_lists.items()}
+        obj.sim_bold = self.sim_bold[key][np.newaxis, ...]
+        obj.sim_states = {k: v[key][np.newaxis, ...] for k, v in self.sim_states.items()}
+        if obj.do_fc:
+            obj.sim_fc_trils = self.sim_fc_trils[key][np.newaxis, ...]
+            if obj.do_fcd:
+                obj.sim_fcd_trils = self.sim_fcd_trils[key][np.newaxis, ...]
+        obj.N = 1
+        return obj
+
+    @property
+    def _to_clear(self):  # base.py:1030-1044
+        names = ["sim_bold", "sim_fc_trils", "sim_fcd_trils", "sim_states", "_sim_states", "_noise",
+                 "_shuffled_nodes", "_shuffled_ts"]
+        return [n for n in names if hasattr(self, n)]
+
+    def clear(self):  # base.py:1046-1053
+        """Drops the simulation outputs."""
+        for name in self._to_clear:
+            if hasattr(self, name):
+                delattr(self, name)
+
+    def _problem_init(self, problem):  # base.py:1055-1065
+        """BNMProblem initialisation hook (nothing by default)."""
+
+    def _problem_evaluate(self, problem, X, out, *args, **kwargs):  # base.py:1067-1082
+        """BNMProblem evaluation hook (nothing by default)."""
+
     def score(self, emp_fc_tril=None, emp_fcd_tril=None, emp_bold=None, force_cpu=False, usable_mem=None):
         """Goodness-of-fit terms per simulation (base.py:1084-1207), computed on the GPU."""
         if emp_bold is not None:
@@ -306,6 +396,30 @@ class rWWSimGroup(SimGroup):
             self.fic_failed = self._global_bools[1]
             self.fic_ntrials = self._global_ints[0]
             self.param_lists["wIE"] = self._regional_params[2].reshape(self.N, -1)
+
+    @property
+    def _to_clear(self):  # rww.py:153-162
+        names = super()._to_clear + ["fic_unstable", "fic_failed", "fic_ntrials"]
+        return [n for n in names if hasattr(self, n)]
+
+    def _problem_init(self, problem):  # rww.py:254-271
+        """Rejects wIE as a free regional parameter under FIC and adds the FIC
+        penalty as an objective of multi-objective problems."""
+        if self.do_fic and "wIE" in problem.het_params:
+            raise ValueError("In rWW wIE should not be specified as a heterogeneous parameter when FIC is done")
+        if problem.multiobj and self.do_fic and self.fic_penalty_scale > 0:
+            problem.obj_names.append("-fic_penalty")
+            problem.n_obj += 1
+
+    def _problem_evaluate(self, problem, X, out, *args, **kwargs):  # rww.py:273-291
+        """Adds the FIC penalty of the last scores to the cost (a column of its
+        own for multi-objective problems)."""
+        scores = kwargs["scores"][-1]
+        if self.do_fic and self.fic_penalty_scale > 0:
+            if problem.multiobj:
+                out["F"] = np.concatenate([out["F"], -scores.loc[:, ["-fic_penalty"]].values], axis=1)
+            else:
+                out["F"] -= scores.loc[:, "-fic_penalty"].values
 
     def score(self, emp_fc_tril=None, emp_fcd_tril=None, emp_bold=None, **kwargs):  # rww.py:180-234
         scores = super().score(emp_fc_tril, emp_fcd_tril, emp_bold, **kwargs)

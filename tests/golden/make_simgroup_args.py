@@ -77,6 +77,9 @@ CASES = {
                                           sim_seed=3), 2, {"G": [0.2, 0.4]}, {}),
     "rwwex": ("rWWExSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
                                     do_fc=False, do_fcd=False, gof_terms=[]), 2, {"G": [0.2, 0.4]}, {}),
+    "rww_hemi": ("rWWSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
+                                     exc_interhemispheric=True, states_ts=True, fic_penalty_scale=1.0), 3,
+                 {"G": [0.2, 0.4, 0.6]}, {}),
     "rww_child": ("rWWSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
                                       do_fic=False), 2, {"G": [0.2, 0.4]}, {}),
 }
@@ -119,7 +122,7 @@ def build(simmod, name, sc_seed=1, N=None):
 
 
 # cases whose run() is answered by fake_outputs() and then scored
-SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi")
+SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi", "rww_hemi")
 N_EMP_FCD = 12
 
 
@@ -134,7 +137,7 @@ def fake_outputs(args, n_state, n_noise=1):
     bold_len = args[16] // args[17]
     out = {"init_time": 0.0, "run_time": 0.0,
            "sim_bold": rng.normal(size=(N, bold_len * nodes)),
-           "_sim_states": rng.uniform(1.0, 5.0, (n_state, N, nodes)),
+           "_sim_states": rng.uniform(1.0, 5.0, (n_state, N, (args[16] // args[18] if args[9] else 1) * nodes)),
            "_global_bools": (rng.random((2, N)) < 0.5),
            "_global_ints": rng.integers(0, 5, (1, N)).astype(np.intc)}
     if args[10]:  # noise_out
@@ -146,7 +149,7 @@ def fake_outputs(args, n_state, n_noise=1):
         out["_shuffled_nodes"] = np.stack([rng.permutation(nodes) for _ in range(reps)]).astype(np.intc)
         out["_shuffled_ts"] = np.stack([rng.permutation(seg) for _ in range(reps)]).astype(np.intc)
     if cfg["do_fc"] == "1":
-        fc = rng.uniform(-1, 1, (N, nodes * (nodes - 1) // 2))
+        fc = rng.uniform(-1, 1, (N, n_pairs(nodes, cfg["exc_interhemispheric"] == "1")))
         if N > 1:
             fc[1] = np.nan
         out["sim_fc_trils"] = fc
@@ -155,9 +158,57 @@ def fake_outputs(args, n_state, n_noise=1):
     return out
 
 
-def empirical(nodes):
+def n_pairs(nodes, exc_interhemispheric):
+    h = nodes // 2
+    return 2 * (h * (h - 1) // 2) if exc_interhemispheric else nodes * (nodes - 1) // 2
+
+
+def empirical(sg):
     rng = np.random.default_rng(77)
-    return rng.uniform(-1, 1, nodes * (nodes - 1) // 2), rng.uniform(-1, 1, N_EMP_FCD)
+    return rng.uniform(-1, 1, n_pairs(sg.nodes, sg.exc_interhemispheric)), rng.uniform(-1, 1, N_EMP_FCD)
+
+
+def problem_hooks(grp, scores):
+    """What the group's BNMProblem hooks (base.py:1055-1082, rww.py:254-291) do
+    to a single- and a multi-objective problem and its cost."""
+    res = {}
+    for multi in (False, True):
+        prob = types.SimpleNamespace(het_params=["w_p"], multiobj=multi, obj_names=["+fc_corr"], n_obj=1)
+        grp._problem_init(prob)
+        F = np.arange(grp.N, dtype=float)
+        out = {"F": F[:, None].copy() if multi else F.copy()}
+        grp._problem_evaluate(prob, None, out, scores=[scores])
+        res[f"obj_names_{int(multi)}"] = np.array(json.dumps(prob.obj_names))
+        res[f"n_obj_{int(multi)}"] = np.asarray(prob.n_obj)
+        res[f"F_{int(multi)}"] = np.asarray(out["F"], dtype=float)
+    return res
+
+
+def helpers(grp):
+    """Outputs of the group's result helpers (base.py:820-1053)."""
+    res = {}
+    avg = grp.get_state_averages()
+    res["state_avg_cols"] = np.array(json.dumps(list(avg.columns)))
+    res["state_avg"] = avg.to_numpy(dtype=float)
+    if grp.do_fc:
+        for i in (0, grp.N - 1):
+            res[f"sim_fc_{i}"] = grp.get_sim_fc(i)
+        if grp.do_fcd:
+            res["sim_fcd_0"] = grp.get_sim_fcd(0)
+    sl = grp.slice(grp.N - 1)
+    res["slice_N"] = np.asarray(sl.N)
+    res["slice_bold"] = np.asarray(sl.sim_bold)
+    for k, v in sl.param_lists.items():
+        res[f"slice_param_{k}"] = np.asarray(v, dtype=float)
+    for k, v in sl.sim_states.items():
+        res[f"slice_state_{k}"] = np.asarray(v, dtype=float)
+    if sl.do_fc:
+        res["slice_fc"] = np.asarray(sl.sim_fc_trils)
+    cleared = list(grp._to_clear)
+    grp.clear()
+    res["cleared"] = np.array(json.dumps(cleared))
+    res["left"] = np.array(json.dumps([a for a in cleared if hasattr(grp, a)]))
+    return res
 
 
 # empirical-helper cases: (BOLD seed, zeroed volumes, FC kwargs, FCD args and kwargs)
@@ -235,10 +286,12 @@ def main(ref_root):
             noise = np.ascontiguousarray(sg.get_noise())
             out[f"{name}|noise_shape"] = np.asarray(noise.shape)
             out[f"{name}|noise_sha256"] = np.array(hashlib.sha256(noise.tobytes()).hexdigest())
-        emp_fc, emp_fcd = empirical(sg.nodes)
+        emp_fc, emp_fcd = empirical(sg)
         for g, grp in enumerate(getattr(sg, "children", [sg])):
             key = f"{name}|{g}"
             scores = grp.score(emp_fc, emp_fcd)
+            for k, v in problem_hooks(grp, scores).items():
+                out[f"{key}|hook|{k}"] = v
             out[f"{key}|score_columns"] = np.array(json.dumps(sorted(scores.columns)))
             for c in scores.columns:
                 out[f"{key}|score|{c}"] = scores[c].to_numpy(dtype=float)
@@ -247,6 +300,8 @@ def main(ref_root):
                 out[f"{key}|wIE"] = np.asarray(grp.param_lists["wIE"], dtype=float)
                 out[f"{key}|fic_ntrials"] = np.asarray(grp.fic_ntrials)
                 out[f"{key}|fic_failed"] = np.asarray(grp.fic_failed)
+            for k, v in helpers(grp).items():
+                out[f"{key}|helper|{k}"] = v
     import cubnm.utils as refutils
     for name, (seed, zeroed, fc_kw, fcd_args, fcd_kw) in UTIL_CASES.items():
         bold = util_bold(seed, zeroed)

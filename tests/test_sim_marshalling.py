@@ -13,8 +13,10 @@ The fixture also holds the reference's ``score()`` of groups whose run was
 answered by ``fake_outputs()``; the same outputs go through this library's
 ``_process_out`` / ``score`` with the GPU goodness-of-fit call replaced by the
 reference's CPU formulas (``base.py:1164-1188``), so what is compared is the
-output handling, signs, NaN fill, ``+gof``, the rWW FIC penalty and the noise
-reconstruction of ``get_noise``.
+output handling, signs, NaN fill, ``+gof``, the rWW FIC penalty, the noise
+reconstruction of ``get_noise``, the BNMProblem hooks (``_problem_init`` /
+``_problem_evaluate``) and the result helpers (``get_state_averages``,
+``get_sim_fc`` / ``get_sim_fcd``, ``slice``, ``clear``).
 """
 import hashlib
 import json
@@ -105,7 +107,7 @@ def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
         noise = np.ascontiguousarray(sg.get_noise())
         assert noise.shape == tuple(FIXTURE[f"{case}|noise_shape"])
         assert hashlib.sha256(noise.tobytes()).hexdigest() == str(FIXTURE[f"{case}|noise_sha256"])
-    emp_fc, emp_fcd = G.empirical(sg.nodes)
+    emp_fc, emp_fcd = G.empirical(sg)
     for g, grp in enumerate(getattr(sg, "children", [sg])):
         key = f"{case}|{g}"
         with np.errstate(invalid="ignore"):
@@ -119,6 +121,23 @@ def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
             np.testing.assert_array_equal(grp.param_lists["wIE"], FIXTURE[f"{key}|wIE"])
             np.testing.assert_array_equal(grp.fic_ntrials, FIXTURE[f"{key}|fic_ntrials"])
             np.testing.assert_array_equal(grp.fic_failed, FIXTURE[f"{key}|fic_failed"])
+        # BNMProblem hooks, then the result helpers (slice, clear, ...)
+        for part, got in (("hook", G.problem_hooks(grp, scores)), ("helper", G.helpers(grp))):
+            want = sorted(k.split("|", 3)[3] for k in FIXTURE.files if k.startswith(f"{key}|{part}|"))
+            assert sorted(got) == want, part
+            for k, v in got.items():
+                ref = FIXTURE[f"{key}|{part}|{k}"]
+                if ref.dtype.kind == "U":
+                    assert str(v) == str(ref), k
+                else:
+                    np.testing.assert_allclose(np.asarray(v, dtype=float), ref, rtol=1e-12, atol=1e-15, err_msg=k)
+
+
+def test_rww_problem_init_rejects_free_wie_under_fic():
+    import types
+    sg = G.build(sim, "rww_fic")
+    with pytest.raises(ValueError, match="wIE should not be specified"):
+        sg._problem_init(types.SimpleNamespace(het_params=["wIE"], multiobj=False, obj_names=[], n_obj=1))
 
 
 @pytest.mark.parametrize("case", list(G.UTIL_CASES))
