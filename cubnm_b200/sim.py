@@ -13,12 +13,25 @@ the library's GPU kernels.  Plotting / saving helpers (``save``, ``labels``)
 are not part of this path.
 """
 import copy
+import os
 from decimal import Decimal
 
 import numpy as np
 import pandas as pd
 
 from . import core, utils
+
+def _load_matrix(m):
+    """An SC / distance matrix given as an array or as a .txt / .npy path."""
+    if isinstance(m, (str, os.PathLike)):
+        m = str(m)
+        if m.endswith(".txt"):
+            return np.loadtxt(m)
+        if m.endswith(".npy"):
+            return np.load(m)
+        raise ValueError(f"Unsupported matrix file (expected .txt or .npy): {m}")
+    return m
+
 
 WORST_SCORES = {"+fc_corr": -1.0, "-fc_diff": -2.0, "-fc_normec": -1.0, "-fcd_ks": -1.0}
 
@@ -40,7 +53,8 @@ class SimGroup:
                  precision="fp64"):
         if force_cpu:
             raise ValueError("force_cpu is not supported: cubnm_b200 runs the simulations on the GPU")
-        self.sc = np.asarray(sc, dtype=float)
+        self.input_sc = sc
+        self.sc = np.asarray(_load_matrix(sc), dtype=float)  # base.py:209-215
         self.nodes = self.sc.shape[-1]
         self.duration = duration
         self.duration_msec = int(Decimal(str(duration)) * 1000)
@@ -69,18 +83,25 @@ class SimGroup:
         self.sim_verbose = sim_verbose
         self.progress_interval = progress_interval
         self.precision = precision
+        self.input_sc_dist = sc_dist
         if sc_dist is None:
             self.sc_dist = np.zeros((self.nodes, self.nodes))
             self.do_delay = False
-        else:
-            self.sc_dist = np.asarray(sc_dist, dtype=float)
+        else:  # base.py:252-264
+            self.sc_dist = np.asarray(_load_matrix(sc_dist), dtype=float)
             self.do_delay = True
         self.bw_params = bw_params
         p = utils.get_bw_params(bw_params) if isinstance(bw_params, str) else bw_params
         for k in ("k1", "k2", "k3"):
             core.set_const(k, p[k])
         self.param_lists = {k: None for k in self.global_param_names + self.regional_param_names + ["v"]}
-        self.out_dir = out_dir  # where the reference's save() writes; saving is not part of this library
+        # where the reference's save() writes (base.py:269-278); saving is not part of this library
+        self.input_out_dir = out_dir
+        if out_dir == "same":
+            assert isinstance(sc, (str, os.PathLike)), "When `out_dir` is set to 'same' `sc` must be a path-like string"
+            self.out_dir = str(sc).replace(".txt", "").replace(".npy", "")
+        else:
+            self.out_dir = out_dir
         self.last_N = 0
         self.last_config = self.get_config()
         self.it = 0

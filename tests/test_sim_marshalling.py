@@ -158,3 +158,25 @@ def test_bw_params_equal_the_reference(src):
     from cubnm_b200 import utils
     p = utils.get_bw_params(src)
     np.testing.assert_array_equal([p["k1"], p["k2"], p["k3"]], FIXTURE[f"util|bw|{src}"])
+
+
+def test_matrices_from_files(tmp_path, monkeypatch):
+    """sc / sc_dist given as .txt and .npy paths (base.py:209-215, 252-264) and
+    out_dir='same' (base.py:269-276) give the arguments of the array form."""
+    sc, dist = G._sc(1), G._dist(5)
+    np.savetxt(tmp_path / "sc.txt", sc)
+    np.save(tmp_path / "dist.npy", dist)
+    kw = dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2, do_fic=False, force_gpu=True)
+    groups = [sim.rWWSimGroup(sc=sc, sc_dist=dist, **kw),
+              sim.rWWSimGroup(sc=str(tmp_path / "sc.txt"), sc_dist=str(tmp_path / "dist.npy"), out_dir="same", **kw)]
+    assert groups[1].out_dir == str(tmp_path / "sc")
+    got = []
+    for sg in groups:
+        sg.N = 2
+        sg.param_lists["G"] = np.array([0.2, 0.4])
+        sg._set_default_params()
+        got.append(_recorded_args(sg, monkeypatch))
+    for i in G.ARRAY_ARGS:
+        np.testing.assert_allclose(np.asarray(got[1][i]), np.asarray(got[0][i]), rtol=1e-15, atol=0)
+    with pytest.raises(ValueError, match="Unsupported"):
+        sim.rWWSimGroup(sc=str(tmp_path / "sc.csv"), **kw)
