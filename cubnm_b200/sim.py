@@ -53,47 +53,42 @@ class SimGroup:
                  precision="fp64"):
         if force_cpu:
             raise ValueError("force_cpu is not supported: cubnm_b200 runs the simulations on the GPU")
+        # the reference's assignment order (base.py:209-286): the property setters
+        # below derive and check the millisecond / TR-count values from these
         self.input_sc = sc
-        self.sc = np.asarray(_load_matrix(sc), dtype=float)  # base.py:209-215
-        self.nodes = self.sc.shape[-1]
+        self.sc = np.asarray(_load_matrix(sc), dtype=float)
         self.duration = duration
-        self.duration_msec = int(Decimal(str(duration)) * 1000)
         self.TR = TR
-        self.TR_msec = int(TR * 1000)
-        self.states_sampling = TR if states_sampling is None else states_sampling
-        self.states_sampling_msec = int(self.states_sampling * 1000)
         self._dt = Decimal(dt)
         self._bw_dt = Decimal(bw_dt)
-        assert self._bw_dt >= self._dt and self._bw_dt % self._dt == 0, "bw_dt must be a multiple of dt"
-        assert Decimal(self.duration_msec) % self._bw_dt == 0, "duration must be a multiple of bw_dt"
+        self._check_dt()
+        self.states_sampling = states_sampling
         self.states_ts = states_ts
-        self.noise_out = noise_out
         self.gof_terms = list(gof_terms)
         self.do_fc = do_fc
         self.do_fcd = do_fcd
         self.window_size = window_size
         self.window_step = window_step
-        self.window_size_TRs = int(np.round(window_size / (TR * 2))) * 2  # base.py:468-476
-        self.window_step_TRs = int(np.round(window_step / TR))
         self.sim_seed = sim_seed
         self.exc_interhemispheric = exc_interhemispheric
+        self.force_cpu = force_cpu
+        self.force_gpu = force_gpu
         self.bold_remove_s = bold_remove_s
         self.fcd_drop_edges = fcd_drop_edges
-        self.noise_segment_length = duration if noise_segment_length is None else noise_segment_length
+        self.noise_segment_length = noise_segment_length
+        self.noise_out = noise_out
         self.sim_verbose = sim_verbose
         self.progress_interval = progress_interval
         self.precision = precision
+        self.nodes = self.sc.shape[-1]
         self.input_sc_dist = sc_dist
         if sc_dist is None:
             self.sc_dist = np.zeros((self.nodes, self.nodes))
             self.do_delay = False
-        else:  # base.py:252-264
+        else:
             self.sc_dist = np.asarray(_load_matrix(sc_dist), dtype=float)
             self.do_delay = True
         self.bw_params = bw_params
-        p = utils.get_bw_params(bw_params) if isinstance(bw_params, str) else bw_params
-        for k in ("k1", "k2", "k3"):
-            core.set_const(k, p[k])
         self.param_lists = {k: None for k in self.global_param_names + self.regional_param_names + ["v"]}
         # where the reference's save() writes (base.py:269-278); saving is not part of this library
         self.input_out_dir = out_dir
@@ -153,12 +148,109 @@ class SimGroup:
             self.param_lists["v"] = np.zeros(N, dtype=float)
 
     @property
+    def duration(self):
+        return self._duration
+
+    @duration.setter
+    def duration(self, duration):  # base.py:339-352
+        self._duration = duration
+        msec = Decimal(duration) * Decimal(1000)
+        if msec % 1 != 0:
+            raise ValueError(
+                f"Duration {duration} seconds equals {msec} milliseconds, which is not a whole number. Duration "
+                "must be expressible in whole milliseconds, i.e., must not have more than 3 decimal places.")
+        self.duration_msec = int(msec)
+        if hasattr(self, "_noise_segment_length") and self.noise_segment_length is None:
+            self.noise_segment_length = self.duration
+
+    @property
+    def TR(self):
+        return self._TR
+
+    @TR.setter
+    def TR(self, TR):  # base.py:358-367
+        self._TR = TR
+        self.TR_msec = int(TR * 1000)
+        if hasattr(self, "_states_sampling") and (self.states_sampling is None or self.states_sampling == self.TR):
+            self.states_sampling = self.TR
+        if hasattr(self, "_window_size"):
+            self.window_size_TRs = int(np.round(self.window_size / (self.TR * 2))) * 2
+        if hasattr(self, "_window_step"):
+            self.window_step_TRs = int(np.round(self.window_step / self.TR))
+
+    @property
+    def states_sampling(self):
+        return self._states_sampling
+
+    @states_sampling.setter
+    def states_sampling(self, states_sampling):  # base.py:373-387
+        if states_sampling is not None and states_sampling < 0.001:
+            raise ValueError("states_sampling cannot be lower than 0.001s which is model dt")
+        self._states_sampling = self.TR if (hasattr(self, "_TR") and states_sampling is None) else states_sampling
+        self.states_sampling_msec = int(self.states_sampling * 1000)
+
+    @property
+    def noise_segment_length(self):
+        return self._noise_segment_length
+
+    @noise_segment_length.setter
+    def noise_segment_length(self, noise_segment_length):  # base.py:397-402
+        if hasattr(self, "_duration") and noise_segment_length is None:
+            self._noise_segment_length = self.duration
+        else:
+            self._noise_segment_length = noise_segment_length
+
+    @property
     def dt(self):
         return self._dt
+
+    @dt.setter
+    def dt(self, dt):  # base.py:408-411
+        self._dt = Decimal(dt)
+        self._check_dt()
 
     @property
     def bw_dt(self):
         return self._bw_dt
+
+    @bw_dt.setter
+    def bw_dt(self, bw_dt):  # base.py:417-420
+        self._bw_dt = Decimal(bw_dt)
+        self._check_dt()
+
+    def _check_dt(self):  # base.py:524-535
+        assert self.bw_dt >= self.dt, "Ballon-Windkessel dt must be greater than or equal to model dt"
+        assert (self.bw_dt % self.dt) == Decimal(0), "Ballon-Windkessel dt must be divisible by model dt"
+        assert (self.duration_msec % self.bw_dt) == Decimal(0), "Duration must be divisible by Ballon-Windkessel dt"
+
+    @property
+    def bw_params(self):
+        return self._bw_params
+
+    @bw_params.setter
+    def bw_params(self, bw_params):  # base.py:441-447
+        self._bw_params = bw_params
+        p = utils.get_bw_params(bw_params)
+        for k in ("k1", "k2", "k3"):
+            core.set_const(k, p[k])
+
+    @property
+    def window_size(self):
+        return self._window_size
+
+    @window_size.setter
+    def window_size(self, window_size):  # base.py:467-472 (nearest even number of TRs)
+        self._window_size = window_size
+        self.window_size_TRs = int(np.round(window_size / (self.TR * 2))) * 2
+
+    @property
+    def window_step(self):
+        return self._window_step
+
+    @window_step.setter
+    def window_step(self, window_step):  # base.py:478-481
+        self._window_step = window_step
+        self.window_step_TRs = int(np.round(window_step / self.TR))
 
     @property
     def bw_it(self):

@@ -12,9 +12,10 @@ positional arguments (``src/cubnm/sim/base.py:727-750``) and stops the run, and
 regular NVIDIA GPU build (no many-nodes mode); every group is made with
 ``force_gpu=True``.  Nothing is simulated.
 
-Each case of ``CASES`` and ``MULTI`` below is built through
-``build(simmod, case)`` for any module with the reference's SimGroup classes, so
-the test builds the same groups with ``cubnm_b200.sim``.
+Each case of ``CASES``, ``MULTI`` and ``MUTATED`` (settings changed after
+construction) below is built through ``build(simmod, case)`` for any module
+with the reference's SimGroup classes, so the test builds the same groups with
+``cubnm_b200.sim``.
 
 The cases of ``SCORE_CASES`` are run once more with the recorder answering
 ``fake_outputs()`` (no simulation: seeded arrays of the output shapes), then
@@ -94,6 +95,12 @@ MULTI = {
 def build(simmod, name, sc_seed=1, N=None):
     """The SimGroup of case `name` (of ``CASES`` or ``MULTI``), from the classes
     of module `simmod`, with N and its parameters set and the defaults filled in."""
+    if name in MUTATED:
+        base, changes = MUTATED[name]
+        sg = build(simmod, base)
+        for k, v in changes:
+            setattr(sg, k, v)
+        return sg
     if name in MULTI:
         cls, children = MULTI[name]
         kids = [build(simmod, c, seed, n) for c, seed, n in children]
@@ -120,6 +127,13 @@ def build(simmod, name, sc_seed=1, N=None):
     sg._set_default_params()
     return sg
 
+
+# groups whose settings are changed after construction: (case, [(attribute, value), ...])
+MUTATED = {
+    "rww_mutated": ("rww_fic", [("duration", 30), ("TR", 0.5), ("window_step", 3), ("dt", "0.05"),
+                                ("noise_segment_length", None), ("bold_remove_s", 4)]),
+    "wc_mutated": ("wc", [("window_size", 6), ("states_sampling", 2), ("bw_dt", "0.5"), ("duration", 12.5)]),
+}
 
 # cases whose run() is answered by fake_outputs() and then scored
 SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi", "rww_hemi")
@@ -260,7 +274,7 @@ def _reference_sim(ref_root):
 def main(ref_root):
     refsim, rec, Stop = _reference_sim(ref_root)
     out = {}
-    for name in list(CASES) + list(MULTI):
+    for name in list(CASES) + list(MULTI) + list(MUTATED):
         sg = build(refsim, name)
         rec.clear()
         try:
@@ -315,7 +329,7 @@ def main(ref_root):
         p = refutils.get_bw_params(src)
         out[f"util|bw|{src}"] = np.array([p["k1"], p["k2"], p["k3"]])
     np.savez_compressed(OUT, **out)
-    print(f"wrote {OUT}: {len(CASES) + len(MULTI)} cases")
+    print(f"wrote {OUT}: {len(CASES) + len(MULTI) + len(MUTATED)} cases")
 
 
 if __name__ == "__main__":

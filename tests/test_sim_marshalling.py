@@ -51,7 +51,7 @@ def _recorded_args(sg, monkeypatch):
     return rec["args"]
 
 
-@pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI))
+@pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI) + list(G.MUTATED))
 def test_run_arguments_equal_the_reference(case, monkeypatch):
     args = _recorded_args(G.build(sim, case), monkeypatch)
     assert len(args) == 22
@@ -180,3 +180,12 @@ def test_matrices_from_files(tmp_path, monkeypatch):
         np.testing.assert_allclose(np.asarray(got[1][i]), np.asarray(got[0][i]), rtol=1e-15, atol=0)
     with pytest.raises(ValueError, match="Unsupported"):
         sim.rWWSimGroup(sc=str(tmp_path / "sc.csv"), **kw)
+
+
+def test_duration_must_be_whole_milliseconds():
+    """Decimal(duration) as base.py:339-350: a float like 0.1 is not a whole
+    number of milliseconds there, nor here."""
+    with pytest.raises(ValueError, match="whole number"):
+        sim.WCSimGroup(duration=0.1, TR=0.05, sc=G._sc(1), bw_dt="0.1", window_size=0.2, window_step=0.1)
+    sg = sim.WCSimGroup(duration=0.5, TR=0.1, sc=G._sc(1), bw_dt="0.1", window_size=0.2, window_step=0.1)
+    assert sg.duration_msec == 500
