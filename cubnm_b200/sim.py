@@ -19,7 +19,7 @@ from decimal import Decimal
 import numpy as np
 import pandas as pd
 
-from . import core, utils
+from . import __version__, core, utils
 
 def _load_matrix(m):
     """An SC / distance matrix given as an array or as a .txt / .npy path."""
@@ -98,7 +98,7 @@ class SimGroup:
         else:
             self.out_dir = out_dir
         self.last_N = 0
-        self.last_config = self.get_config()
+        self.last_config = self.get_config(for_reinit=True)
         self.it = 0
         self._N = 0
         self.post_init()
@@ -264,15 +264,30 @@ class SimGroup:
     def n_states_samples_remove(self):
         return int(self.bold_remove_s / self.states_sampling)
 
-    def get_config(self):
-        return {
+    @property
+    def use_cpu(self):  # base.py:660-671; there is no CPU path here
+        return False
+
+    def get_config(self, include_N=False, for_reinit=False):  # base.py:581-633
+        """The group's configuration: with `for_reinit` only what requires a new
+        session (memory and noise) when it changes, which run() compares."""
+        config = {
             "duration": self.duration, "TR": self.TR, "nodes": self.nodes, "states_ts": self.states_ts,
             "states_sampling": self.states_sampling, "do_fc": self.do_fc, "do_fcd": self.do_fcd,
+            "window_size": self.window_size, "window_step": self.window_step,
             "window_size_TRs": self.window_size_TRs, "window_step_TRs": self.window_step_TRs,
             "sim_seed": self.sim_seed, "exc_interhemispheric": self.exc_interhemispheric,
+            "force_cpu": self.force_cpu, "force_gpu": self.force_gpu, "hardware_used": "gpu",
             "bold_remove_s": self.bold_remove_s, "fcd_drop_edges": self.fcd_drop_edges,
-            "noise_segment_length": self.noise_segment_length, "precision": self.precision,
+            "noise_segment_length": self.noise_segment_length,
+            "precision": self.precision,  # this library's addition
         }
+        if not for_reinit:
+            config.update({"out_dir": self.input_out_dir, "gof_terms": self.gof_terms, "sc": self.input_sc,
+                           "sc_dist": self.input_sc_dist, "bw_params": self.bw_params, "version": __version__})
+            if include_N:
+                config["N"] = self.N
+        return config
 
     @property
     def _model_config(self):  # base.py:635-657
@@ -324,7 +339,7 @@ class SimGroup:
                 float(self.bw_dt))
 
     def run(self, force_reinit=False):  # base.py:673-766
-        cfg = self.get_config()
+        cfg = self.get_config(for_reinit=True)
         force_reinit = force_reinit or (self.N != self.last_N) or (cfg != self.last_config)
         out = core.run_simulations(*self._run_args(force_reinit))
         self.last_N = self.N
@@ -494,6 +509,13 @@ class rWWSimGroup(SimGroup):
         if self.do_fic:
             self.param_lists["wIE"] = np.zeros((N, self.nodes), dtype=float)
 
+    def get_config(self, *args, **kwargs):  # rww.py:102-112
+        config = super().get_config(*args, **kwargs)
+        config.update({"do_fic": self.do_fic, "max_fic_trials": self.max_fic_trials,
+                       "I_SAMPLING_START": self.I_SAMPLING_START, "I_SAMPLING_END": self.I_SAMPLING_END,
+                       "init_delta": self.init_delta, "fic_penalty_scale": self.fic_penalty_scale})
+        return config
+
     @property
     def _model_config(self):
         cfg = super()._model_config
@@ -596,6 +618,11 @@ class KuramotoSimGroup(SimGroup):
             self.param_lists["init_theta"] = np.tile(rng.uniform(0, 2 * np.pi, self.nodes), (N, 1))
         else:
             self.param_lists["init_theta"] = np.zeros((N, self.nodes), dtype=float)
+
+    def get_config(self, *args, **kwargs):  # kuramoto.py:92-97
+        config = super().get_config(*args, **kwargs)
+        config["random_init_theta"] = self.random_init_theta
+        return config
 
     @property
     def _model_config(self):

@@ -182,6 +182,25 @@ def empirical(sg):
     return rng.uniform(-1, 1, n_pairs(sg.nodes, sg.exc_interhemispheric)), rng.uniform(-1, 1, N_EMP_FCD)
 
 
+def config_record(sg):
+    """get_config(include_N=True) and get_config(for_reinit=True) of a group
+    (base.py:581-633) as JSON: array values by their kind only, the package
+    version by its presence."""
+    def enc(cfg):
+        out = {}
+        for k, v in cfg.items():
+            if isinstance(v, np.ndarray):
+                v = "<array>"
+            elif k == "version":
+                v = "<version>"
+            elif isinstance(v, (np.generic,)):
+                v = v.item()
+            out[k] = v
+        return out
+    return json.dumps({"full": enc(sg.get_config(include_N=True)), "reinit": enc(sg.get_config(for_reinit=True))},
+                      sort_keys=True)
+
+
 def problem_hooks(grp, scores):
     """What the group's BNMProblem hooks (base.py:1055-1082, rww.py:254-291) do
     to a single- and a multi-objective problem and its cost."""
@@ -288,6 +307,7 @@ def main(ref_root):
         meta = {str(i): args[i] for i in range(22) if i not in ARRAY_ARGS and i != 7}
         meta["model_config"] = args[7]
         out[f"{name}|meta"] = np.array(json.dumps(meta, sort_keys=True))
+        out[f"{name}|config"] = np.array(config_record(sg))
     if not hasattr(np, "NaN"):  # the reference's rww.py:220 predates numpy 2
         np.NaN = np.nan
     for name in SCORE_CASES:

@@ -53,7 +53,8 @@ def _recorded_args(sg, monkeypatch):
 
 @pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI) + list(G.MUTATED))
 def test_run_arguments_equal_the_reference(case, monkeypatch):
-    args = _recorded_args(G.build(sim, case), monkeypatch)
+    sg = G.build(sim, case)
+    args = _recorded_args(sg, monkeypatch)
     assert len(args) == 22
     for i in G.ARRAY_ARGS:
         ref = FIXTURE[f"{case}|{i}"]
@@ -67,6 +68,11 @@ def test_run_arguments_equal_the_reference(case, monkeypatch):
     cfg = dict(args[7])
     assert cfg.pop("precision") == "fp64"
     assert cfg == ref_cfg
+    # get_config (base.py:581-633), without the precision key this library adds
+    got = json.loads(G.config_record(sg))
+    for part in got.values():
+        assert part.pop("precision") == "fp64"
+    assert got == json.loads(str(FIXTURE[f"{case}|config"]))
 
 
 def test_fc_fcd_and_gof_term_checks():
