@@ -453,7 +453,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         throw Err(CBNM_ERR_UNSUPPORTED, "use_cpu is not supported: this library runs the simulations on the GPU only");
     Cfg c;
     build_cfg(c, a, md);
-    if (c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this build");
+    if (c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this library");
     if (c.do_fc && !o->sim_fc_trils) throw Err(CBNM_ERR_ARG, "do_fc is set but sim_fc_trils is null");
     if (c.do_fcd && !o->sim_fcd_trils) throw Err(CBNM_ERR_ARG, "do_fcd is set but sim_fcd_trils is null");
     if (c.ext_out && !o->sim_states) throw Err(CBNM_ERR_ARG, "ext_out is set but sim_states is null");
@@ -899,7 +899,7 @@ static AdjPlan adjoint_plan(const cbnm_run_args *a, int segment_steps) {
     build_cfg(P.c, a, *P.md);
     P.c.fp32 = true;
     if (P.c.do_fic) throw Err(CBNM_ERR_UNSUPPORTED, "gradients need do_fic = 0 (wIE given)");
-    if (P.c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this build");
+    if (P.c.nodes > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "more than 1024 nodes is not supported by this library");
     if (segment_steps <= 0 || segment_steps % P.c.inner_it != 0)
         throw Err(CBNM_ERR_ARG, "segment_steps must be a positive multiple of bw_dt / dt = " + std::to_string(P.c.inner_it));
     const int N = P.c.n_sims, n = P.c.nodes;

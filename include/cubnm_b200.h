@@ -44,7 +44,7 @@ extern "C" {
 #define CBNM_ERR_CONFIG 3       /* configuration rejected (e.g. no FC windows) */
 #define CBNM_ERR_CUDA 4         /* CUDA runtime error; message starts with "CUDA Error" */
 #define CBNM_ERR_TIMEOUT 5      /* a bounded device-side wait gave up */
-#define CBNM_ERR_UNSUPPORTED 6  /* request outside what this build implements */
+#define CBNM_ERR_UNSUPPORTED 6  /* request outside what this library implements */
 
 /* Arguments of one run; positional arguments of core.cpp:202-225 in order. */
 typedef struct cbnm_run_args {
