@@ -442,6 +442,14 @@ static void fill_sizes(const Cfg &c, const ModelDesc &md, cbnm_sizes *sz) {
 // ---------------------------------------------------------------- run
 // sp: the session to run on; null = the process's default session, opened once
 // the arguments have been validated (so argument errors come before device errors)
+// Touches one byte per 4 KB page of a host output buffer so that its pages are
+// mapped (and zeroed by the OS) now, while the GPU is still computing, rather
+// than inside the device-to-host copy into it.  The copy overwrites every byte.
+static void prefault_host(void *p, size_t bytes) {
+    volatile unsigned char *c = static_cast<volatile unsigned char *>(p);
+    for (size_t i = 0; i < bytes; i += 4096) c[i] = 0;
+}
+
 static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
     const double t_begin = now_s();
     check_args(a);
@@ -765,6 +773,12 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         ++launches;
     }
     CK(cudaEventRecord(S.ev[2], S.st));
+    if (!device_io) {  // the integrator runs asynchronously: map the host output pages meanwhile
+        prefault_host(o->sim_bold, sizeof(double) * bold_n);
+        if (c.do_fc) prefault_host(o->sim_fc_trils, sizeof(double) * (size_t)N * c.n_pairs);
+        if (c.do_fc && c.do_fcd) prefault_host(o->sim_fcd_trils, sizeof(double) * (size_t)N * c.n_window_pairs);
+        if (c.ext_out) prefault_host(o->sim_states, sizeof(double) * states_n);
+    }
 
     // ---- FC / FCD (bnm.cu:809-942), in chunks that bound the window-FC scratch
     double *d_fc = nullptr, *d_fcd = nullptr;
