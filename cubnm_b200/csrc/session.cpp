@@ -1012,12 +1012,22 @@ static void gof_impl(const double *sim_fc, int n_sims, int n_pairs, const double
                      int n_wp, const double *emp_fcd, int n_emp_fcd, double *fc_corr, double *fc_diff,
                      double *fc_normec, double *fcd_ks) {
     if (n_sims <= 0) return;
+    const bool want_fc = sim_fc && emp_fc && n_pairs > 0 && (fc_corr || fc_diff || fc_normec);
+    const bool want_ks = sim_fcd && emp_fcd && n_wp > 0 && n_emp_fcd > 0 && fcd_ks;
+    if (want_ks) {
+        size_t m1p = 1;  // the KS kernel sorts one simulation's FCD, padded to a power of two, in shared memory
+        while (m1p < (size_t)n_wp) m1p <<= 1;
+        if (sizeof(double) * m1p > gof_ks_smem_limit()) {
+            size_t max_pairs = 1;
+            while (sizeof(double) * (max_pairs << 1) <= gof_ks_smem_limit()) max_pairs <<= 1;
+            throw Err(CBNM_ERR_UNSUPPORTED, "FCD too long for the KS kernel: " + std::to_string(n_wp) +
+                                                " window pairs per simulation (at most " + std::to_string(max_pairs) + ")");
+        }
+    }
     Session &S = session();
     GofArgs g;
     std::memset(&g, 0, sizeof(g));
     g.n_sims = n_sims; g.n_pairs = n_pairs; g.n_wp = n_wp; g.n_emp_fcd = n_emp_fcd;
-    const bool want_fc = sim_fc && emp_fc && n_pairs > 0 && (fc_corr || fc_diff || fc_normec);
-    const bool want_ks = sim_fcd && emp_fcd && n_wp > 0 && n_emp_fcd > 0 && fcd_ks;
     double *d_out = (double *)S.g_out.ensure(sizeof(double) * 4 * n_sims);
     if (want_fc) {
         double m = 0;
@@ -1037,8 +1047,6 @@ static void gof_impl(const double *sim_fc, int n_sims, int n_pairs, const double
     }
     std::vector<double> emp_sorted;
     if (want_ks) {
-        if (sizeof(double) * (size_t)n_wp > gof_ks_smem_limit())
-            throw Err(CBNM_ERR_UNSUPPORTED, "FCD too long for the KS kernel");
         emp_sorted.assign(emp_fcd, emp_fcd + n_emp_fcd);
         std::sort(emp_sorted.begin(), emp_sorted.end());
         S.g_simfcd.ensure(sizeof(double) * (size_t)n_sims * n_wp);

@@ -97,3 +97,11 @@ def test_config_errors(golden):
 def test_wrong_argument_count_returns_none(capsys):
     assert core.run_simulations("rWW") is None
     assert "parsing" in capsys.readouterr().err
+
+
+def test_gof_rejects_fcd_longer_than_the_ks_kernel_holds():
+    """The KS kernel sorts one simulation's FCD, padded to a power of two, in
+    shared memory; longer FCDs are refused before any device work."""
+    from cubnm_b200 import utils
+    with pytest.raises(RuntimeError, match=r"FCD too long for the KS kernel: 16385 .*at most 16384"):
+        utils.gof(sim_fcd_trils=np.zeros((2, 16385)), emp_fcd_tril=np.zeros(10), terms=["fcd_ks"])
