@@ -105,3 +105,12 @@ def test_gof_rejects_fcd_longer_than_the_ks_kernel_holds():
     from cubnm_b200 import utils
     with pytest.raises(RuntimeError, match=r"FCD too long for the KS kernel: 16385 .*at most 16384"):
         utils.gof(sim_fcd_trils=np.zeros((2, 16385)), emp_fcd_tril=np.zeros(10), terms=["fcd_ks"])
+
+
+def test_run_batch_argument_errors():
+    """An empty batch and a group without the 22 arguments are refused before
+    any device work."""
+    with pytest.raises(RuntimeError, match="no groups"):
+        core.run_batch([])
+    with pytest.raises(TypeError, match="22"):
+        core.run_batch([("rWW",)])
