@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(1024) k_adj_forward(const AdjArgs A) {
         }
         if (act) bw_step(bx, bf, bnu, bq, (double)s[M::BOLDV], a.bw);
         if ((bw_i + 1) % a.bold_tr_iters == 0) {
-            if (act)
+            if (act && bold_i < a.bold_len)  // no slot for a sample past bold_len
                 bold[(size_t)bold_i * n + j] =
                     a.bw.V_0 * (a.bw.k1 * (1 - bq) + a.bw.k2 * (1 - bq / bnu) + a.bw.k3 * (1 - bnu));
             bold_i++;
@@ -222,8 +222,9 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs A) {
                 const double z = (double)scr_z[(size_t)b * n + j];
                 double x1b = x0, f1b = f0, nu1 = nu0, q1 = q0;
                 bw_step(x1b, f1b, nu1, q1, z, c);
-                if ((bw_i + 1) % a.bold_tr_iters == 0) {  // BOLD = V0 (k1 (1-q) + k2 (1-q/nu) + k3 (1-nu))
-                    const double gb = dbold[(size_t)((bw_i + 1) / a.bold_tr_iters - 1) * n + j];
+                const int vol = (bw_i + 1) / a.bold_tr_iters - 1;
+                if ((bw_i + 1) % a.bold_tr_iters == 0 && vol < a.bold_len) {  // BOLD = V0 (k1 (1-q) + k2 (1-q/nu) + k3 (1-nu))
+                    const double gb = dbold[(size_t)vol * n + j];
                     lq += gb * c.V_0 * (-c.k1 - c.k2 / nu1);
                     lnu += gb * c.V_0 * (c.k2 * q1 / (nu1 * nu1) - c.k3);
                 }

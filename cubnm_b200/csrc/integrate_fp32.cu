@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                 w[8 * u + 4] = (uint32_t)__double2loint(nu[u]); w[8 * u + 5] = (uint32_t)__double2hiint(nu[u]);
                 w[8 * u + 6] = (uint32_t)__double2loint(q[u]); w[8 * u + 7] = (uint32_t)__double2hiint(q[u]);
                 const int sim = sims[2 * pr + u];
-                if (tr && act && sim >= 0)
+                if (tr && act && sim >= 0 && bi < a.bold_len)  // no slot for a sample past bold_len
                     a.bold[(size_t)sim * a.bold_len * n + (size_t)bi * n + j] =
                         bw.V0k1 * (1 - q[u]) + bw.V0k2 * (1 - q[u] / nu[u]) + bw.V0k3 * (1 - nu[u]);
             }
@@ -728,8 +728,10 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                                 if (sim < 0) continue;
                                 for (int v = 0; v < M::NOUT; ++v) {
                                     const double ov = u ? o[v].y : o[v].x;
-                                    if (a.states_ts)
-                                        a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = ov;
+                                    if (a.states_ts) {
+                                        if (states_i < a.states_len)
+                                            a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = ov;
+                                    }
                                     else if (states_i >= a.n_states_samples_remove)
                                         a.states[((size_t)v * a.n_sims + sim) * ext + j] += ov;
                                 }

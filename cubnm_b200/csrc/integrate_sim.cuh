@@ -193,7 +193,9 @@ __global__ void __launch_bounds__(MAXT) k_integrate_sim(const IntegrateArgs a) {
         }
         if (act) bw_step(bx, bf, bnu, bq, (double)s[M::BOLDV], a.bw);
         if ((bw_i + 1) % a.bold_tr_iters == 0) {  // bnm.cpp:316-335
-            if (act)
+            // the truncated iteration counts (bw_it, bold_tr_iters) can give one more
+            // sample than bold_len for some TR / bw_dt; that sample has no slot
+            if (act && bold_i < a.bold_len)
                 bold[(size_t)bold_i * n + j] =
                     a.bw.V_0 * (a.bw.k1 * (1 - bq) + a.bw.k2 * (1 - bq / bnu) + a.bw.k3 * (1 - bnu));
             bold_i++;
@@ -201,9 +203,10 @@ __global__ void __launch_bounds__(MAXT) k_integrate_sim(const IntegrateArgs a) {
         if (a.ext_out && (bw_i + 1) % a.states_sampling_iters == 0) {  // bnm.cpp:337-355
             if (act) {
                 if (a.states_ts) {
+                    if (states_i < a.states_len)
 #pragma unroll
-                    for (int v = 0; v < M::NS; ++v)
-                        a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = (double)s[v];
+                        for (int v = 0; v < M::NS; ++v)
+                            a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = (double)s[v];
                 } else if (states_i >= a.n_states_samples_remove) {
 #pragma unroll
                     for (int v = 0; v < M::NS; ++v) ssum[v] += (double)s[v];

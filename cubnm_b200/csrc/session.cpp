@@ -245,8 +245,9 @@ static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
 // bnm.cu:1240-1256 + utils.cpp:74-95.  The values come from std::mt19937 and
 // libstdc++'s std::normal_distribution<double>; the node and time shuffles are
 // restated explicitly: the bounded draw is the division-based rejection method
-// and two swap positions come from one draw in [0, (i+1)(i+2)), which is what
-// the libstdc++ that produced the reference's stored outputs does.
+// and, while n^2 fits in the generator's 32-bit range, two swap positions come
+// from one draw in [0, (i+1)(i+2)) (otherwise one draw in [0, i] per element),
+// which is what the libstdc++ that produced the reference's stored outputs does.
 static uint64_t bounded_draw(std::mt19937 &g, uint64_t range_max) {
     const uint64_t urng_range = 0xffffffffULL;
     const uint64_t span = range_max + 1, scaling = urng_range / span, past = span * scaling;
@@ -257,6 +258,10 @@ static uint64_t bounded_draw(std::mt19937 &g, uint64_t range_max) {
 static void shuffle_positions(std::vector<int> &v, std::mt19937 &g) {
     const size_t n = v.size();
     if (n < 2) return;
+    if (0xffffffffULL / n < n) {  // n^2 exceeds the generator's range: one draw in [0, i] per element
+        for (size_t i = 1; i < n; ++i) std::swap(v[i], v[bounded_draw(g, i)]);
+        return;
+    }
     size_t i = 1;
     if (n % 2 == 0) { std::swap(v[i], v[bounded_draw(g, 1)]); ++i; }
     while (i != n) {

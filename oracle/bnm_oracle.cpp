@@ -548,6 +548,10 @@ static uint64_t bounded_draw(std::mt19937 &g, uint64_t range_max) {  // uniform 
 static void shuffle_ref(std::vector<int> &v, std::mt19937 &g) {
     const uint64_t n = v.size();
     if (n < 2) return;
+    if (0xffffffffULL / n < n) {  // n^2 exceeds the generator's range: one draw in [0, i] per element
+        for (size_t i = 1; i < n; ++i) std::swap(v[i], v[bounded_draw(g, i)]);
+        return;
+    }
     size_t i = 1;
     if (n % 2 == 0) { std::swap(v[i], v[bounded_draw(g, 1)]); ++i; }
     while (i != n) {  // positions for elements i and i+1 from one draw in [0, (i+1)(i+2))
@@ -686,14 +690,16 @@ static void simulate(int sim, const RunCfg &c, const cbnm_run_args *a, const dou
         }
         for (int j = 0; j < n; ++j) bw_step(bx[j], bf[j], bnu[j], bq[j], s[(size_t)j * M::NS + M::BOLDV], bwc);
         if ((bw_i + 1) % c.BOLD_TR_iters == 0) {  // bnm.cpp:316-335
-            for (int j = 0; j < n; ++j)
+            // truncated iteration counts can give one sample past bold_len, which has no slot
+            for (int j = 0; j < n && bold_i < c.bold_len; ++j)
                 bold[(size_t)bold_i * n + j] = bwc.V_0 * (bwc.k1 * (1 - bq[j]) + bwc.k2 * (1 - bq[j] / bnu[j]) + bwc.k3 * (1 - bnu[j]));
             bold_i++;
         }
         if (c.ext_out && (bw_i + 1) % c.states_sampling_iters == 0) {  // bnm.cpp:337-355
             for (int j = 0; j < n; ++j) {
                 if (c.states_ts) {
-                    for (int v = 0; v < M::NS; ++v) st(v)[(size_t)states_i * n + j] = s[(size_t)j * M::NS + v];
+                    if (states_i < c.states_len)
+                        for (int v = 0; v < M::NS; ++v) st(v)[(size_t)states_i * n + j] = s[(size_t)j * M::NS + v];
                 } else if (states_i >= c.n_states_samples_remove) {
                     for (int v = 0; v < M::NS; ++v) st(v)[j] += s[(size_t)j * M::NS + v];
                 }
