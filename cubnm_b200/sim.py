@@ -314,9 +314,9 @@ class SimGroup:
             if (not missing) or cur is None or np.asarray(cur).shape[0] != self.N:
                 if v is None:
                     raise ValueError(f"Parameter {param} does not have a default value and must be set")
-                if param in self.global_param_names or param == "v":
+                if param in self.global_param_names:
                     self.param_lists[param] = np.repeat(v, self.N).astype(float)
-                else:
+                else:  # including the default velocity, (N, nodes) as base.py:567-575; the core reads v[:N]
                     if param == "wIE" and getattr(self, "do_fic", False):
                         continue
                     self.param_lists[param] = np.full((self.N, self.nodes), v, dtype=float)

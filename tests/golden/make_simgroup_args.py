@@ -81,6 +81,8 @@ CASES = {
     "rww_hemi": ("rWWSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
                                      exc_interhemispheric=True, states_ts=True, fic_penalty_scale=1.0), 3,
                  {"G": [0.2, 0.4, 0.6]}, {}),
+    "wc_delay_default_v": ("WCSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
+                                              sc_dist="dist"), 2, {"G": [0.5, 1.5]}, {}),
     "rww_child": ("rWWSimGroup", dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2,
                                       do_fic=False), 2, {"G": [0.2, 0.4]}, {}),
 }
