@@ -12,10 +12,10 @@ positional arguments (``src/cubnm/sim/base.py:727-750``) and stops the run, and
 regular NVIDIA GPU build (no many-nodes mode); every group is made with
 ``force_gpu=True``.  Nothing is simulated.
 
-Each case of ``CASES``, ``MULTI`` and ``MUTATED`` (settings changed after
-construction) below is built through ``build(simmod, case)`` for any module
-with the reference's SimGroup classes, so the test builds the same groups with
-``cubnm_b200.sim``.
+Each case of ``CASES``, ``MULTI``, ``MUTATED`` (settings changed after
+construction) and ``RANDOM`` (60 seeded random groups) below is built through
+``build(simmod, case)`` for any module with the reference's SimGroup classes,
+so the test builds the same groups with ``cubnm_b200.sim``.
 
 The cases of ``SCORE_CASES`` are run once more with the recorder answering
 ``fake_outputs()`` (no simulation: seeded arrays of the output shapes), then
@@ -97,6 +97,8 @@ MULTI = {
 def build(simmod, name, sc_seed=1, N=None):
     """The SimGroup of case `name` (of ``CASES`` or ``MULTI``), from the classes
     of module `simmod`, with N and its parameters set and the defaults filled in."""
+    if name in RANDOM:
+        return build_random(simmod, name)
     if name in MUTATED:
         base, changes = MUTATED[name]
         sg = build(simmod, base)
@@ -126,6 +128,47 @@ def build(simmod, name, sc_seed=1, N=None):
             sg.param_lists[p] = v
     for k, v in extra.items():
         setattr(sg, k, np.asarray(v))
+    sg._set_default_params()
+    return sg
+
+
+def random_cases(n=60, seed=5):
+    """n seeded random groups over model, TR, windows, dt, sampling, noise segment,
+    delays and FIC options: {name: (class, constructor kwargs, N)}, JSON-able
+    (sc_dist given as the flag "dist")."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for i in range(n):
+        cls = str(rng.choice(["rWWSimGroup", "WCSimGroup", "JRSimGroup", "KuramotoSimGroup", "rWWExSimGroup"]))
+        kw = dict(duration=int(rng.choice([10, 30, 60])), TR=float(rng.choice([0.5, 0.72, 1, 2])),
+                  window_size=int(rng.choice([4, 10, 30])), window_step=int(rng.choice([1, 2, 5])),
+                  bold_remove_s=int(rng.choice([0, 2, 5])), dt=str(rng.choice(["0.1", "0.5", "1.0"])), bw_dt="1.0",
+                  sim_seed=int(rng.integers(0, 5)), states_ts=bool(rng.integers(0, 2)),
+                  noise_out=bool(rng.integers(0, 2)), noise_segment_length=[None, 5, 30][int(rng.integers(0, 3))],
+                  fcd_drop_edges=bool(rng.integers(0, 2)))
+        if rng.random() < 0.3:
+            kw["states_sampling"] = float(rng.choice([0.5, 1, 2]))
+        if cls == "rWWSimGroup":
+            kw["do_fic"] = bool(rng.integers(0, 2))
+            kw["max_fic_trials"] = int(rng.choice([0, 3]))
+        if rng.random() < 0.3:
+            kw["sc_dist"] = "dist"
+        out[f"random_{i:02d}"] = (cls, kw, int(rng.integers(1, 4)))
+    return out
+
+
+RANDOM = random_cases()
+
+
+def build_random(simmod, name):
+    """The group of random case `name` with G = linspace(0.1, 1, N) and defaults."""
+    cls, kw, N = RANDOM[name]
+    kw = dict(kw, force_gpu=True, sc=_sc(2))
+    if kw.get("sc_dist") == "dist":
+        kw["sc_dist"] = _dist(3)
+    sg = getattr(simmod, cls)(**kw)
+    sg.N = N
+    sg.param_lists["G"] = np.linspace(0.1, 1, N)
     sg._set_default_params()
     return sg
 
@@ -295,7 +338,7 @@ def _reference_sim(ref_root):
 def main(ref_root):
     refsim, rec, Stop = _reference_sim(ref_root)
     out = {}
-    for name in list(CASES) + list(MULTI) + list(MUTATED):
+    for name in list(CASES) + list(MULTI) + list(MUTATED) + list(RANDOM):
         sg = build(refsim, name)
         rec.clear()
         try:
@@ -351,7 +394,7 @@ def main(ref_root):
         p = refutils.get_bw_params(src)
         out[f"util|bw|{src}"] = np.array([p["k1"], p["k2"], p["k3"]])
     np.savez_compressed(OUT, **out)
-    print(f"wrote {OUT}: {len(CASES) + len(MULTI) + len(MUTATED)} cases")
+    print(f"wrote {OUT}: {len(CASES) + len(MULTI) + len(MUTATED) + len(RANDOM)} cases")
 
 
 if __name__ == "__main__":

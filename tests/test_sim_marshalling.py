@@ -51,7 +51,7 @@ def _recorded_args(sg, monkeypatch):
     return rec["args"]
 
 
-@pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI) + list(G.MUTATED))
+@pytest.mark.parametrize("case", list(G.CASES) + list(G.MULTI) + list(G.MUTATED) + list(G.RANDOM))
 def test_run_arguments_equal_the_reference(case, monkeypatch):
     sg = G.build(sim, case)
     args = _recorded_args(sg, monkeypatch)
