@@ -99,6 +99,13 @@ def build(simmod, name, sc_seed=1, N=None):
     of module `simmod`, with N and its parameters set and the defaults filled in."""
     if name in RANDOM:
         return build_random(simmod, name)
+    if name in RANDOM_SCORE:
+        cls, kw, N = RANDOM_SCORE[name]
+        sg = getattr(simmod, cls)(**dict(kw, force_gpu=True, sc=_sc(1)))
+        sg.N = N
+        sg.param_lists["G"] = np.linspace(0.1, 1, N)
+        sg._set_default_params()
+        return sg
     if name in MUTATED:
         base, changes = MUTATED[name]
         sg = build(simmod, base)
@@ -160,6 +167,27 @@ def random_cases(n=60, seed=5):
 RANDOM = random_cases()
 
 
+def random_score_cases(n=20, seed=9):
+    """n seeded random rWW / WC groups for scoring: random subsets of the GOF
+    terms, FIC penalty scales, state time series and hemisphere exclusion."""
+    rng = np.random.default_rng(seed)
+    terms_all = ["+fc_corr", "-fc_diff", "-fc_normec", "-fcd_ks"]
+    out = {}
+    for i in range(n):
+        cls = str(rng.choice(["rWWSimGroup", "WCSimGroup"]))
+        terms = [str(t) for t in rng.choice(terms_all, size=int(rng.integers(1, 5)), replace=False)]
+        kw = dict(duration=10, TR=1, window_size=4, window_step=2, bold_remove_s=2, gof_terms=terms,
+                  states_ts=bool(rng.integers(0, 2)), exc_interhemispheric=bool(rng.integers(0, 2)))
+        if cls == "rWWSimGroup":
+            kw["do_fic"] = bool(rng.integers(0, 2))
+            kw["fic_penalty_scale"] = float(rng.choice([0.0, 0.5, 2.0]))
+        out[f"score_random_{i:02d}"] = (cls, kw, int(rng.integers(1, 5)))
+    return out
+
+
+RANDOM_SCORE = random_score_cases()
+
+
 def build_random(simmod, name):
     """The group of random case `name` with G = linspace(0.1, 1, N) and defaults."""
     cls, kw, N = RANDOM[name]
@@ -181,7 +209,7 @@ MUTATED = {
 }
 
 # cases whose run() is answered by fake_outputs() and then scored
-SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi", "rww_hemi")
+SCORE_CASES = ("rww_fic", "rww_delay", "wc", "rww_multi", "rww_hemi")  # + RANDOM_SCORE, defined below
 N_EMP_FCD = 12
 
 
@@ -355,7 +383,7 @@ def main(ref_root):
         out[f"{name}|config"] = np.array(config_record(sg))
     if not hasattr(np, "NaN"):  # the reference's rww.py:220 predates numpy 2
         np.NaN = np.nan
-    for name in SCORE_CASES:
+    for name in list(SCORE_CASES) + list(RANDOM_SCORE):
         sg = build(refsim, name)
         rec.clear()
         rec["answer"] = True
@@ -379,8 +407,9 @@ def main(ref_root):
                 out[f"{key}|wIE"] = np.asarray(grp.param_lists["wIE"], dtype=float)
                 out[f"{key}|fic_ntrials"] = np.asarray(grp.fic_ntrials)
                 out[f"{key}|fic_failed"] = np.asarray(grp.fic_failed)
-            for k, v in helpers(grp).items():
-                out[f"{key}|helper|{k}"] = v
+            if name in SCORE_CASES:
+                for k, v in helpers(grp).items():
+                    out[f"{key}|helper|{k}"] = v
     import cubnm.utils as refutils
     for name, (seed, zeroed, fc_kw, fcd_args, fcd_kw) in UTIL_CASES.items():
         bold = util_bold(seed, zeroed)

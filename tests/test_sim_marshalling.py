@@ -103,7 +103,7 @@ def _cpu_gof(sim_fc_trils=None, emp_fc_tril=None, sim_fcd_trils=None, emp_fcd_tr
     return out
 
 
-@pytest.mark.parametrize("case", G.SCORE_CASES)
+@pytest.mark.parametrize("case", list(G.SCORE_CASES) + list(G.RANDOM_SCORE))
 def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
     sg = G.build(sim, case)
     monkeypatch.setattr(sim.core, "run_simulations", lambda *a: G.fake_outputs(a, len(sg.state_names), sg.n_noise))
@@ -128,7 +128,10 @@ def test_processed_outputs_and_scores_equal_the_reference(case, monkeypatch):
             np.testing.assert_array_equal(grp.fic_ntrials, FIXTURE[f"{key}|fic_ntrials"])
             np.testing.assert_array_equal(grp.fic_failed, FIXTURE[f"{key}|fic_failed"])
         # BNMProblem hooks, then the result helpers (slice, clear, ...)
-        for part, got in (("hook", G.problem_hooks(grp, scores)), ("helper", G.helpers(grp))):
+        parts = [("hook", G.problem_hooks(grp, scores))]
+        if case in G.SCORE_CASES:
+            parts.append(("helper", G.helpers(grp)))
+        for part, got in parts:
             want = sorted(k.split("|", 3)[3] for k in FIXTURE.files if k.startswith(f"{key}|{part}|"))
             assert sorted(got) == want, part
             for k, v in got.items():
