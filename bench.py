@@ -33,9 +33,8 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-for p in (ROOT, os.path.join(ROOT, "tests")):
-    if p not in sys.path:
-        sys.path.insert(0, p)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
@@ -52,7 +51,7 @@ UNIT = "sims*sim-s/s"
 
 
 def workload_args(n_sims, duration_s, precision, seed):
-    import cases
+    from cubnm_b200 import synthetic
     rng = np.random.default_rng(1000 + seed)
     G = rng.uniform(0.001, 10, n_sims)
     wp = rng.uniform(0, 2, n_sims)
@@ -60,7 +59,7 @@ def workload_args(n_sims, duration_s, precision, seed):
     # the headline case removes 30 s of BOLD before FC; short profiling runs keep 3/4 of it
     remove = 30 if duration_s >= 60 else duration_s // 4
     window = 10 if duration_s - remove > 12 else 2
-    return list(cases.synthetic_args("rWW", N=n_sims, nodes=NODES, duration_s=duration_s, seed=0, G=G, w_p=wp,
+    return list(synthetic.synthetic_args("rWW", N=n_sims, nodes=NODES, duration_s=duration_s, seed=0, G=G, w_p=wp,
                                      J_N=jn, precision=precision, window_size=window, window_step=2,
                                      bold_remove_s=remove))
 
@@ -147,7 +146,7 @@ def run_ours(opts, rank, world, local_rank):
     import torch
     from cubnm_b200 import _abi, core, utils
     from cubnm_b200._lib import lib, check
-    import cases
+    from cubnm_b200 import synthetic
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -199,7 +198,7 @@ def run_ours(opts, rank, world, local_rank):
     value = world * n_sims * opts.duration / (ms / 1e3)
 
     # end to end through the host C ABI (host buffers; copies inside the timed region) + GOF scoring
-    emp = cases.synthetic_emp_bold(NODES, opts.duration, 7)
+    emp = synthetic.synthetic_emp_bold(NODES, opts.duration, 7)
     emp_fc = utils.calculate_fc(emp)
     emp_fcd = utils.calculate_fcd(emp, 10 if opts.duration >= 16 else 2, 2)
     host_args = [a.copy() if isinstance(a, np.ndarray) else a for a in args]

@@ -196,6 +196,8 @@ int fc_fcd_noalloc(const double *bold, int n_sims, int bold_len, int nodes, int 
     NoAllocArgs a;
     a.nodes = nodes; a.bold_len = bold_len; a.n_vols_remove = n_vols_remove; a.exc_inter = exc_inter ? 1 : 0;
     a.n_pairs = nodes * (nodes - 1) / 2 - (a.exc_inter ? (nodes / 2) * (nodes / 2) : 0);
+    // two nodes with exc_interhemispheric leave no pair (one node per hemisphere)
+    if (a.n_pairs < 1) return fail(msg, cap, 3, "no node pairs for FC (exc_interhemispheric with 2 nodes)");
     a.n_windows = 0; a.n_window_pairs = 0; a.win_first = 0; a.win_step = 1; a.win_half = 0; a.sim_begin = 0;
     a.bold = bold; a.fc = fc; a.fcd = fcd; a.wfc = nullptr;
     int max_T = corr_len;

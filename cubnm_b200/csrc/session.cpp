@@ -216,6 +216,9 @@ static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
             if (c.nodes % 2 != 0) throw Err(CBNM_ERR_CONFIG, "exc_interhemispheric is set but number of nodes is not even");
             c.n_pairs -= (c.nodes / 2) * (c.nodes / 2);
         }
+        if (c.n_pairs < 1)  // one node, or two with exc_interhemispheric: nothing to correlate
+            throw Err(CBNM_ERR_CONFIG, "no node pairs for FC (" + std::to_string(c.nodes) + " nodes" +
+                                           (c.exc_inter ? ", exc_interhemispheric)" : ")"));
         if (c.do_fcd) {  // utils.cpp:21-52
             int first = c.drop_edges ? c.window_size / 2 : 0;
             int last = c.drop_edges ? c.corr_len - 1 - c.window_size / 2 : c.corr_len - 1;
@@ -296,6 +299,7 @@ struct DBuf {
 
 struct Session {
     bool ready = false;
+    int dev = -1;                // the device the stream, events and buffers belong to
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8];
     // noise cache (bnm.cu:1207-1215 key)
@@ -320,12 +324,27 @@ static Session *g_sess = nullptr;
 static std::vector<Session *> g_batch;  // one per concurrent worker of cbnm_run_batch
 static cbnm_timing g_last_timing{};     // timings of the last run call (single, batch or adjoint)
 
+// A session belongs to the device that was current when it opened: one device
+// per process, as the reference's process-global model object.  A call made
+// while another device is current fails instead of launching on a foreign
+// stream or reusing another device's buffers; cbnm_reset() releases the session
+// so that the next call opens one on the new device.
 static void open_session(Session &S) {
-    if (S.ready) return;
+    int cur = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (S.ready) {
+        if (e != cudaSuccess) throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: ") + cudaGetErrorString(e));
+        if (cur != S.dev)
+            throw Err(CBNM_ERR_CUDA, "CUDA Error: the session was opened on device " + std::to_string(S.dev) +
+                                         " but device " + std::to_string(cur) +
+                                         " is current; call cbnm_reset() before switching devices");
+        return;
+    }
     int ndev = 0;
-    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e == cudaSuccess) e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0)
         throw Err(CBNM_ERR_CUDA, std::string("CUDA Error: no CUDA device available (") + cudaGetErrorString(e) + ")");
+    S.dev = cur;
     CK(cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking));
     for (auto &ev : S.ev) CK(cudaEventCreate(&ev));
     S.ready = true;
@@ -341,6 +360,9 @@ static void close_session(Session *&p) {
     if (!p) return;
     Session &S = *p;
     if (S.ready) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != S.dev) cudaSetDevice(S.dev);  // free on the device that owns the buffers
         cudaStreamSynchronize(S.st);
         for (DBuf *b : {&S.d_noise, &S.d_noise_f32, &S.d_sh_nodes, &S.d_sh_ts, &S.d_sc, &S.d_sc_f32, &S.d_sc_idx,
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
@@ -351,6 +373,7 @@ static void close_session(Session *&p) {
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
         cudaStreamDestroy(S.st);
+        if (cur >= 0 && cur != S.dev) cudaSetDevice(cur);
     }
     delete p;
     p = nullptr;

@@ -27,6 +27,12 @@
  * Thread safety: like the reference (a process-global model object,
  * core.cpp:57-58), the library keeps one session per process; calls must not
  * overlap.  Errors return a non-zero status; cbnm_last_error() describes it.
+ *
+ * Devices: the session (stream, events, device buffers, noise cache) belongs to
+ * the CUDA device that was current at the first call.  Use one device per
+ * process; a run call made while another device is current returns
+ * CBNM_ERR_CUDA.  cbnm_reset() frees the session on its own device, after which
+ * the next call opens a new one on the then-current device.
  */
 #ifndef CUBNM_B200_H
 #define CUBNM_B200_H

@@ -92,6 +92,11 @@ def test_config_errors(golden):
     args[7] = {"do_fc": 1}
     with pytest.raises(TypeError):
         core.run_simulations(*args)
+    # two nodes, one per hemisphere: no FC pair (rejected before any device work)
+    two = list(cases.synthetic_args("rWW", N=2, nodes=2, duration_s=60))
+    two[7] = dict(two[7], exc_interhemispheric="1")
+    with pytest.raises(RuntimeError, match="no node pairs"):
+        core.run_simulations(*two)
 
 
 def test_wrong_argument_count_returns_none(capsys):

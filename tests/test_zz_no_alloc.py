@@ -72,6 +72,32 @@ def test_noalloc_matches_run_simulations_twice(name):
 
 
 @pytest.mark.gpu
+def test_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: after a first call (which may load
+    the module holding the scratch), further calls leave the device's free memory
+    unchanged -- here a call over several scratch chunks, twice."""
+    import torch
+    N, nodes, dur, ws, step, rm, exc = CASES["several_scratch_chunks"]
+    ref = _simulate(N, nodes, dur, ws, step, rm, exc)
+    L, f = _noalloc()
+    bold = torch.from_numpy(np.ascontiguousarray(ref["sim_bold"]).reshape(N, -1)).to("cuda:0")
+    bold_len = bold.shape[1] // nodes
+    fc = torch.empty(ref["sim_fc_trils"].shape, dtype=torch.float64, device="cuda:0")
+    fcd = torch.empty(ref["sim_fcd_trils"].shape, dtype=torch.float64, device="cuda:0")
+    call = lambda: f(bold.data_ptr(), N, bold_len, nodes, rm, ws, step, 1, int(exc), fc.data_ptr(),  # noqa: E731
+                     fcd.data_ptr(), None)
+    assert call() == 0, L.cbnm_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        assert call() == 0, L.cbnm_last_error()
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (free0, free1)
+    np.testing.assert_allclose(fcd.cpu().numpy(), ref["sim_fcd_trils"], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.gpu
 def test_noalloc_fc_only_after_fcd_call():
     import torch
     N, nodes, dur, ws, step, rm, exc = CASES["default_windows"]
@@ -107,5 +133,8 @@ def test_noalloc_rejects_bad_configs():
     assert f(fake, 4, 60, 100, 59, 10, 2, 1, 0, fake, fake, None) == 3      # one volume left for FC
     assert f(fake, 4, 60, 99, 30, 10, 2, 1, 1, fake, fake, None) == 3       # odd nodes with exc_interhemispheric
     assert f(fake, 4, 60, 100, 30, 10, 0, 1, 0, fake, fake, None) == 3      # window_step 0
+    assert f(fake, 4, 60, 2, 30, 10, 2, 1, 1, fake, fake, None) == 3        # 2 nodes, one per hemisphere: no pair
+    assert "no node pairs" in L.cbnm_last_error().decode()
+    assert f(fake, 4, 60, 2, 30, 10, 2, 1, 1, fake, None, None) == 3        # the same for FC only
     assert f(None, 4, 60, 100, 30, 10, 2, 1, 0, fake, fake, None) == 1      # no BOLD
     assert "BOLD" in L.cbnm_last_error().decode() or "bold" in L.cbnm_last_error().decode()
