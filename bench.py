@@ -221,14 +221,18 @@ def run_ours(opts, rank, world, local_rank):
 
     # FP64 reference-precision path on one full wave, same metric
     fp64 = None
+    line_errors = None
     if not opts.skip_fp64:
         n64 = min(n_sims, 4736)
         a64 = workload_args(n64, opts.duration, "fp64", seed=rank)
-        core.run_simulations(*a64)
+        o64 = core.run_simulations(*a64)
         t64 = core.last_timing()
         fp32_sub = workload_args(n64, opts.duration, opts.precision, seed=rank)
-        core.run_simulations(*fp32_sub)
+        o32 = core.run_simulations(*fp32_sub)
         t32 = core.last_timing()
+        err = precision_error(o64, o32, emp_fc, emp_fcd)
+        err["sims"] = n64
+        line_errors = err
         # the same subset with the reference's default rWW setting, analytical FIC on
         # (wIE solved per node on the GPU before the integrator), end to end
         fic_sub = workload_args(n64, opts.duration, opts.precision, seed=rank)
@@ -278,6 +282,7 @@ def run_ours(opts, rank, world, local_rank):
         "gpu_launches": launches,
         "kernel_ms": {"integrate": float(np.mean(integ_ms)), "fc_fcd": float(np.mean(fc_ms))},
         "fp64_path": fp64,
+        "error_vs_fp64": line_errors,
         "roofline": roof,
         "clocks": ck,
     }
@@ -290,11 +295,33 @@ def run_ours(opts, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+# Bounds of the mixed-precision mode against the FP64 run of the same inputs and noise
+FC_BOUND, GOF_BOUND = 2e-3, 1e-3
+
+
+def precision_error(o64, o32, emp_fc, emp_fcd):
+    """Largest |FP32 - FP64| of BOLD, FC, FCD and of every GOF term over a batch."""
+    from cubnm_b200 import utils
+    g64 = utils.gof(o64["sim_fc_trils"], emp_fc, o64["sim_fcd_trils"], emp_fcd)
+    g32 = utils.gof(o32["sim_fc_trils"], emp_fc, o32["sim_fcd_trils"], emp_fcd)
+    d = lambda a, b: float(np.nanmax(np.abs(np.asarray(a) - np.asarray(b))))  # noqa: E731
+    err = {"bold": d(o64["sim_bold"], o32["sim_bold"]), "fc": d(o64["sim_fc_trils"], o32["sim_fc_trils"]),
+           "fcd": d(o64["sim_fcd_trils"], o32["sim_fcd_trils"]),
+           "gof": {k: d(g64[k], g32[k]) for k in g64}}
+    err["within_bounds"] = bool(err["fc"] <= FC_BOUND and max(err["gof"].values()) <= GOF_BOUND)
+    err["bounds"] = {"fc": FC_BOUND, "gof": GOF_BOUND}
+    if not err["within_bounds"]:
+        raise SystemExit(f"FP32 path outside its error bounds against FP64: {err}")
+    return err
+
+
 def cpu_baseline(opts, sample=None):
-    """The reference's CPU algorithm (oracle restatement, OpenMP over sims, all host threads)."""
+    """The reference's CPU algorithm (oracle restatement, OpenMP over sims, all host
+    threads) on a sample of the workload: 16 simulations per thread (256 on 16
+    threads), so that the OpenMP split is even and the sample is ~1 minute."""
     from oracle import oracle
     threads = oracle.num_threads()
-    sample = sample or max(16, 2 * threads)
+    sample = sample or 16 * threads
     args = workload_args(sample, opts.duration, "fp64", seed=0)
     t0 = time.perf_counter()
     oracle.run_simulations(*args)
@@ -305,11 +332,22 @@ def cpu_baseline(opts, sample=None):
 
 
 def run_reference(opts, rank, world):
+    """The reference arm: the reference's CPU algorithm (the oracle port), all host
+    threads.  Each step is a sample of the workload whose size is set from an untimed
+    probe so that the K timed steps take about --ref-budget seconds together (default
+    240; at least two simulations per thread, at most 512 simulations)."""
     if rank != 0:
         return
     from oracle import oracle
     threads = oracle.num_threads()
-    sample = max(16, 2 * threads)
+    probe = 2 * threads
+    args = workload_args(probe, opts.duration, "fp64", seed=0)
+    t0 = time.perf_counter()
+    oracle.run_simulations(*[a.copy() if isinstance(a, np.ndarray) else a for a in args])
+    per_sim = (time.perf_counter() - t0) / probe
+    budget_s = opts.ref_budget / max(1, opts.steps)
+    sample = int(budget_s / per_sim) // threads * threads
+    sample = max(2 * threads, min(512, sample))
     args = workload_args(sample, opts.duration, "fp64", seed=0)
     for _ in range(max(0, min(opts.warmup, 1))):
         oracle.run_simulations(*[a.copy() if isinstance(a, np.ndarray) else a for a in args])
@@ -340,6 +378,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per integrator launch")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="reference arm: seconds the timed CPU steps should take together")
     opts = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -7,7 +7,8 @@ import subprocess
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-CMD = [sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0", "--duration", "20"]
+CMD = [sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0", "--duration", "20",
+       "--ref-budget", "2"]
 
 
 def _run(env_extra):
@@ -27,6 +28,7 @@ def test_reference_arm_prints_the_contract_line():
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["config"]["sample_sims_per_step"] >= 2 * line["cpu_baseline"]["cores"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
 
