@@ -14,6 +14,13 @@ struct BWConst {
     double ialpha, itau, oneminrho, dt_itau, V_0_k1, V_0_k2, V_0_k3;
 };
 
+// Balloon-Windkessel constants in the form the FP32 tensor-core kernels use (FP64
+// step with series for the powers, tc_common.cuh): filled on the host.
+struct BWFast {
+    double dt, kappa, y, dt_itau, ialpha, irho, log2_omr, ln_omr, omr, V0k1, V0k2, V0k3;
+    double binom[13];            // C(1/alpha, k), k = 0..12
+};
+
 // Model constants, computed on the host exactly as the reference's
 // init_constants(dt) does (src/ext/models/<model>.cpp).
 struct RWWK {
@@ -77,7 +84,11 @@ struct IntegrateArgs {
     int n_tiles;
     int tile_width;              // FP32 kernel: simulations per tile (16 or 32)
     double bw_binom[13];         // FP32 kernel: binomial coefficients C(1/alpha, k), k = 0..12
+    BWFast bwf;                  // two-tile kernel: Balloon-Windkessel constants
+    alignas(8) float k32[24];    // two-tile kernel: the model's FP32 constants (M::K)
     int *status;                 // device status word (0 = ok)
+    double *bw_scratch;          // two-tile kernel: per-CTA Balloon-Windkessel state (pp_bw_scratch_bytes)
+    int pp_grid;                 // two-tile kernel: CTAs launched (the scratch holds this many)
     // Sparse coupling (per-simulation kernels), ELLPACK by target node: entry q of
     // node j at [q * nodes + j]; ell_k entries per node, zero-weight padding last.
     // One entry = the SC weight packed with the source's offset into the ring
@@ -116,6 +127,11 @@ cudaError_t launch_integrate_fp64(int model, const IntegrateArgs &a, cudaStream_
 cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStream_t st);  // FP32, one CTA per simulation
 bool fp32_supported(int model, int nodes, bool has_delay);
+// Two-tile tensor-core kernel (integrate_pp.cu): rWW, no delays, <= 128 nodes.
+// Work items: [n_tiles][1 + 64] = SC index, then 32 simulation ids per half (-1 = empty).
+bool pp_supported(int model, int nodes, bool has_delay);
+size_t pp_bw_scratch_bytes(int nodes, int grid);
+cudaError_t launch_integrate_pp(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
 int fp32_tile_for(int nodes);  // simulations per FP32 tile for a node count
 // rWW analytical FIC (fic.cu): wIE written into regional row 2 in place.
 struct FicArgs {

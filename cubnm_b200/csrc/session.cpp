@@ -10,6 +10,7 @@
 // stream, CUDA-event timings, status codes instead of exceptions, a cached
 // session keyed on everything that changes the noise (as bnm.cu:1207-1215).
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -28,6 +29,7 @@
 
 #include "../../include/cubnm_b200.h"
 #include "engine.h"
+#include "tc_common.cuh"
 
 namespace cbnm {
 
@@ -314,7 +316,7 @@ struct Session {
     // run buffers
     DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
-    DBuf d_tiles, d_sct_f32, d_ell_pk;
+    DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr;
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -368,7 +370,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_pk,
+                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -476,6 +478,51 @@ static void fill_sizes(const Cfg &c, const ModelDesc &md, cbnm_sizes *sz) {
 static void prefault_host(void *p, size_t bytes) {
     volatile unsigned char *c = static_cast<volatile unsigned char *>(p);
     for (size_t i = 0; i < bytes; i += 4096) c[i] = 0;
+}
+
+static int sm_count() {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+// Work items of the two-tile kernel from 32-simulation tiles ([n][33]: SC index,
+// simulation ids): items [m][65] = SC index, half 0, half 1 (-1 = empty).  Tiles
+// of one SC are paired; an odd tile of an SC runs as a single.  The items are
+// spread over `sms` CTAs in rounds (item w runs in round w / grid); while a round
+// would be partly empty, pairs are split into singles (one half idle, a shorter
+// step) until every round is full or no pair is left, singles last.
+static std::vector<int> pair_tiles(const std::vector<int> &tiles, int n_tiles, int sms, int *n_items, int *grid) {
+    constexpr int W = 33;
+    std::vector<std::array<int, 2>> pairs, singles;
+    for (int t = 0; t < n_tiles;) {
+        if (t + 1 < n_tiles && tiles[(size_t)t * W] == tiles[(size_t)(t + 1) * W]) {
+            pairs.push_back({t, t + 1});
+            t += 2;
+        } else {
+            singles.push_back({t, -1});
+            t += 1;
+        }
+    }
+    auto count = [&] { return (int)(pairs.size() + singles.size()); };
+    const int g = std::max(1, sms);
+    while (!pairs.empty() && (count() < g || count() % g != 0)) {  // every CTA busy in every round
+        const auto pq = pairs.back();
+        pairs.pop_back();
+        singles.insert(singles.begin(), {{pq[0], -1}, {pq[1], -1}});
+    }
+    std::vector<int> out;
+    out.reserve((size_t)count() * 65);
+    for (const auto *v : {&pairs, &singles})
+        for (const auto &pq : *v) {
+            out.push_back(tiles[(size_t)pq[0] * W]);
+            for (int h = 0; h < 2; ++h)
+                for (int i = 0; i < 32; ++i) out.push_back(pq[h] >= 0 ? tiles[(size_t)pq[h] * W + 1 + i] : -1);
+        }
+    *n_items = count();
+    *grid = std::max(1, std::min(sms, count()));
+    return out;
 }
 
 static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
@@ -662,6 +709,19 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         }
     }
     ia.K = make_constants(md.id, c.dt);
+    {  // the two-tile kernel reads these from its parameter space
+        BWFast &f = ia.bwf;
+        f.dt = ia.bw.dt; f.kappa = ia.bw.kappa; f.y = ia.bw.y; f.dt_itau = ia.bw.dt_itau; f.ialpha = ia.bw.ialpha;
+        f.irho = 1.0 / ia.bw.rho; f.log2_omr = std::log2(ia.bw.oneminrho); f.ln_omr = std::log(ia.bw.oneminrho);
+        f.omr = ia.bw.oneminrho;
+        f.V0k1 = ia.bw.V_0 * ia.bw.k1; f.V0k2 = ia.bw.V_0 * ia.bw.k2; f.V0k3 = ia.bw.V_0 * ia.bw.k3;
+        std::copy(ia.bw_binom, ia.bw_binom + 13, f.binom);
+        if (md.id == MODEL_RWW) {
+            const RWW32::K k = RWW32::make(ia.K);
+            static_assert(sizeof(k) <= sizeof(ia.k32), "FP32 constants");
+            std::memcpy(ia.k32, &k, sizeof(k));
+        }
+    }
     ia.sim_begin = 0;
     ia.n_regional = md.n_regional;
     ia.status = d_status;
@@ -759,9 +819,13 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
             CK(cudaStreamSynchronize(S.st));  // host vectors go out of scope
         }
     }
+    // rWW on the tensor cores: the two-tile kernel unless CBNM_FP32_TC=v5 selects the
+    // single-tile one
+    const char *tc_kind = std::getenv("CBNM_FP32_TC");
+    const bool use_pp = use_tc && pp_supported(md.id, n, has_delay) && !(tc_kind && std::string(tc_kind) == "v5");
     if (use_tc) {
         // tiles of simulations that share one SC
-        const int TN = fp32_tile_for(n);
+        const int TN = use_pp ? 32 : fp32_tile_for(n);
         ia.tile_width = TN;
         std::vector<int> sc_of(N);
         if (device_io) {
@@ -785,12 +849,15 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
             for (; cnt < TN; ++cnt) tiles.push_back(-1);
         }
         ia.n_tiles = (int)(tiles.size() / (TN + 1));
+        if (use_pp) tiles = pair_tiles(tiles, ia.n_tiles, sm_count(), &ia.n_tiles, &ia.pp_grid);
         S.d_tiles.ensure(sizeof(int) * tiles.size());
         CK(cudaMemcpyAsync(S.d_tiles.p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, S.st));
         ia.tiles = S.d_tiles.as<int>();
+        if (use_pp) ia.bw_scratch = (double *)S.d_bw_scr.ensure(pp_bw_scratch_bytes(n, ia.pp_grid));
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));
-        CK(launch_integrate_fp32(md.id, ia, S.st, &launches));
+        if (use_pp) CK(launch_integrate_pp(md.id, ia, S.st, &launches));
+        else CK(launch_integrate_fp32(md.id, ia, S.st, &launches));
     } else if (c.fp32) {
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));

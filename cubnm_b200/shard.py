@@ -6,8 +6,8 @@ and the duration, not on which simulations a process runs.  So a batch is cut
 into contiguous shards of simulations, each rank runs its shard through the
 single-GPU entry point on its own device, and the outputs are gathered.  The
 gathered result equals the one-GPU result of the whole batch, simulation by
-simulation.  The only collectives are the gather of outputs at the end and a
-MAX of timings; none sits on the data path.
+simulation.  The only collectives are the gather of outputs at the end (to one
+rank by default) and a MAX of timings; none sits on the data path.
 
 The reference runs a batch on one GPU (src/cubnm/sim/base.py:673-766 calls
 cubnm.core.run_simulations once); this module adds the multi-GPU split behind
@@ -82,14 +82,17 @@ def merge_outputs(parts):
     return out
 
 
-def run_sharded(args, runner=None, group=None, weights=None):
+def run_sharded(args, runner=None, group=None, weights=None, dst=0):
     """Runs the batch described by the reference's 22 arguments across the ranks of
     ``group`` (torch.distributed must be initialised; each rank on its own GPU).
 
-    Every rank returns the merged output dict of the whole batch.  Parameters the
+    The shards' outputs are gathered on rank ``dst`` only (one pickled message per
+    other rank), which returns the merged output dict of the whole batch; the other
+    ranks return None.  ``dst=None`` gathers on every rank instead.  Parameters the
     run modifies (rWW FIC writes wIE back, src/ext/core.cpp:437-450) are written
-    back into the caller's ``regional_params`` on every rank.  ``runner`` defaults
-    to :func:`cubnm_b200.core.run_simulations`; it receives the shard's 22 arguments.
+    back into ``regional_params`` on the ranks that receive the outputs.
+    ``runner`` defaults to :func:`cubnm_b200.core.run_simulations`; it receives
+    the shard's 22 arguments.
     """
     import torch.distributed as dist
     if runner is None:
@@ -105,8 +108,15 @@ def run_sharded(args, runner=None, group=None, weights=None):
     if out is not None:
         out = dict(out)
         out["_regional_params_shard"] = mine[A_REGIONAL]
-    parts = [None] * world
-    dist.all_gather_object(parts, out, group=group)
+    if dst is None:
+        parts = [None] * world
+        dist.all_gather_object(parts, out, group=group)
+    else:
+        dst_global = dist.get_global_rank(group, dst) if group is not None else dst
+        parts = [None] * world if rank == dst else None
+        dist.gather_object(out, parts, dst=dst_global, group=group)
+        if rank != dst:
+            return None
     reg = args[A_REGIONAL]
     if isinstance(reg, np.ndarray) and reg.dtype == np.float64 and reg.flags.c_contiguous:
         full = reg.reshape(-1, n, nodes)

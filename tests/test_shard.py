@@ -51,15 +51,18 @@ def test_slice_and_merge_reproduce_the_whole_batch():
     _assert_same(shard.merge_outputs(parts), whole)
 
 
-def _worker(rank, world, port, path):
+def _worker(rank, world, port, path, dst):
     import torch.distributed as dist
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
         args = _small_batch()
-        out = shard.run_sharded(args, runner=oracle.run_simulations)
+        out = shard.run_sharded(args, runner=oracle.run_simulations, dst=dst)
         slowest = shard.max_over_ranks(float(rank + 1))
-        np.savez(os.path.join(path, f"rank{rank}.npz"), wie=args[5][2], slowest=slowest,
-                 **{k: np.asarray(v) for k, v in out.items()})
+        if out is None:
+            np.savez(os.path.join(path, f"rank{rank}.npz"), none=1, slowest=slowest)
+        else:
+            np.savez(os.path.join(path, f"rank{rank}.npz"), wie=args[5][2], slowest=slowest,
+                     **{k: np.asarray(v) for k, v in out.items()})
     finally:
         dist.destroy_process_group()
 
@@ -70,14 +73,20 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def test_run_sharded_over_gloo_world2():
+@pytest.mark.parametrize("dst", [0, None])
+def test_run_sharded_over_gloo_world2(dst):
+    """dst=0: rank 0 receives the merged batch (and the FIC write-back), rank 1 None;
+    dst=None: every rank receives it."""
     import torch.multiprocessing as mp
     args = _small_batch()
     whole = oracle.run_simulations(*args)  # writes the analytical-FIC wIE into args[5]
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_worker, args=(2, _free_port(), d), nprocs=2, join=True, start_method="spawn")
+        mp.start_processes(_worker, args=(2, _free_port(), d, dst), nprocs=2, join=True, start_method="spawn")
         for r in range(2):
             got = dict(np.load(os.path.join(d, f"rank{r}.npz")))
             assert float(got.pop("slowest")) == 2.0
-            np.testing.assert_array_equal(got.pop("wie"), args[5][2])  # FIC write-back on every rank
+            if dst is not None and r != dst:
+                assert "none" in got
+                continue
+            np.testing.assert_array_equal(got.pop("wie"), args[5][2])  # FIC write-back
             _assert_same({k: v for k, v in got.items()}, {k: np.asarray(v) for k, v in whole.items()})
