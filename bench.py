@@ -366,6 +366,276 @@ def run_reference(opts, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- other configurations
+# --config c0|c2|c3|c4 runs the other workloads of the benchmark plan with the same
+# JSON contract.  c0 is run at full size.  c2 and c4 are too long for a routine run at
+# full size (c2: 8,192 simulations of 60-900 s, ~3.8e6 simulated s; c4: 2,048 x 300 s
+# at 1,000 nodes): their durations are divided by --scale (the line says by how much);
+# simulations, node counts, densities and delays are as specified.  c3's gradient is one
+# forward + backward of the adjoint on --grad-sims simulations at the full duration.
+C2_NODES = (68, 100, 200, 400)
+C2_DURATIONS = (60, 300, 600, 900)
+
+
+def c2_groups(scale, precision="fp32", sims_per_group=512):
+    """Uneven batch: 8,192 rWW simulations over node counts x durations (16 groups of
+    512), delays from 3-D points in a 70-mm sphere x 1.3 at 6 m/s, SC at 20 %, regional
+    w_p = w_p0 + w_p1 map.  Durations divided by `scale`."""
+    from cubnm_b200 import synthetic
+    groups = []
+    for gi, (nodes, dur) in enumerate([(n, d) for n in C2_NODES for d in C2_DURATIONS]):
+        d = max(2, int(round(dur / scale)))
+        rng = np.random.default_rng(500 + gi)
+        N = sims_per_group
+        remove = min(10, d // 4)
+        window = 30 if d - remove >= 60 else 2
+        step = 5 if window == 30 else 1
+        a = list(synthetic.synthetic_args("rWW", N=N, nodes=nodes, duration_s=d, seed=nodes, density=0.2,
+                                          G=rng.uniform(0.001, 10, N), J_N=rng.uniform(0.001, 0.5, N),
+                                          precision=precision, window_size=window, window_step=step,
+                                          bold_remove_s=remove))
+        fmap = np.random.default_rng(nodes + 100).standard_normal(nodes)
+        a[5][0] = (rng.uniform(0, 2, N)[:, None] + rng.uniform(-1, 1, N)[:, None] * fmap[None, :]).ravel()
+        a[3] = np.ascontiguousarray(synthetic.synthetic_lengths(nodes, nodes).ravel())
+        a[6] = np.full(N, 6.0)
+        a[11] = True
+        groups.append(a)
+    return groups
+
+
+def c4_args(n_sims, duration_s, precision="fp32"):
+    """Wilson-Cowan, 1,000 nodes, SC at 10 % (lognormal, row-sum normalised: a sparse
+    gather), delays as c2 at 6 m/s, noise sigma 0.01, G ~ U[0.001, 5]."""
+    from cubnm_b200 import synthetic
+    nodes = 1000
+    rng = np.random.default_rng(44)
+    a = list(synthetic.synthetic_args("WC", N=n_sims, nodes=nodes, duration_s=duration_s, seed=4, density=0.1,
+                                      G=rng.uniform(0.001, 5, n_sims), precision=precision,
+                                      window_size=30 if duration_s >= 90 else 2,
+                                      window_step=5 if duration_s >= 90 else 1,
+                                      bold_remove_s=min(30, duration_s // 4)))
+    reg = a[5].reshape(8, n_sims, nodes)
+    reg[6] = 0.01   # sigma_E
+    reg[7] = 0.01   # sigma_I
+    a[3] = np.ascontiguousarray(synthetic.synthetic_lengths(nodes, 4).ravel())
+    a[6] = np.full(n_sims, 6.0)
+    a[11] = True
+    return a
+
+
+def _copy_args(args):
+    return [x.copy() if isinstance(x, np.ndarray) else x for x in args]
+
+
+def _oracle_sample(args, sample, duration_s=None):
+    """The reference CPU algorithm (oracle) on the first `sample` simulations of a
+    group (optionally a shorter duration): sims x sim-s per s and the wall time."""
+    from oracle import oracle
+    from cubnm_b200 import shard
+    a = shard.slice_args(args, 0, sample)
+    if duration_s is not None:
+        a[16] = int(duration_s * 1000)
+        a[7] = dict(a[7], do_fc="0", do_fcd="0")
+    t0 = time.perf_counter()
+    oracle.run_simulations(*a)
+    el = time.perf_counter() - t0
+    return sample * a[16] / 1000 / el, el
+
+
+def run_config(opts):
+    import torch
+    from cubnm_b200 import _abi, core, synthetic, utils
+    from cubnm_b200._lib import lib, check
+    from oracle import oracle
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = lib()
+    threads = oracle.num_threads()
+    st = torch.cuda.current_stream()
+    clocks = Clocks(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]))
+    extra = {}
+
+    def device_runner(args):
+        sizes = _abi.Sizes()
+        check(L.cbnm_query_sizes(C.byref(_abi.Prepared(*args).args), C.byref(sizes)))
+        bufs, prep, outs = device_buffers(torch, args, sizes, dev)
+
+        def step():
+            check(L.cbnm_run_simulations_device(C.byref(prep.args), C.byref(outs)))
+            return core.last_timing()
+        return step, bufs
+
+    if opts.config == "c0":
+        G, wp, jn = synthetic.rww_grid()
+        args = list(synthetic.synthetic_args("rWW", N=100, nodes=100, duration_s=60, seed=0, G=G, w_p=wp, J_N=jn,
+                                             precision="fp64"))
+        workload = "README grid: rWW 4x5x5 = 100 sims, 100 nodes, 60 s, FP64, FC+FCD w10/s2, no FIC"
+        sim_s = 100 * 60
+        step, _ = device_runner(args)
+        for _ in range(opts.warmup):
+            step()
+        clocks.start()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        launches = 0
+        for _ in range(opts.steps):
+            launches += step()["kernel_launches"]
+        e1.record(st)
+        torch.cuda.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1) / opts.steps
+        t0 = time.perf_counter()
+        out = core.run_simulations(*_copy_args(args))
+        e2e_s = time.perf_counter() - t0
+        tm = core.last_timing()
+        e2e = {"value": sim_s / e2e_s, "unit": UNIT, "h2d_bytes_per_step": tm["h2d_bytes"],
+               "d2h_bytes_per_step": tm["d2h_bytes"]}
+        # parity with the reference's CPU algorithm on the same inputs and noise
+        t0 = time.perf_counter()
+        ref = oracle.run_simulations(*_copy_args(args))
+        cpu_s = time.perf_counter() - t0
+        rel = {k: float(np.max(np.abs(out[k] - ref[k]) / (np.abs(ref[k]) + 1e-12)))
+               for k in ("sim_bold", "sim_fc_trils", "sim_fcd_trils")}
+        extra["parity_vs_oracle_max_rel"] = rel
+        cpu = {"value": sim_s / cpu_s, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"the whole workload (100 sims x 60 s), {cpu_s:.1f} s wall"}
+        value, dtype = sim_s / (ms / 1e3), "f64"
+        roof = None
+    elif opts.config == "c2":
+        scale = opts.scale or 15.0
+        groups = c2_groups(scale)
+        sim_s = sum(g[14] * g[16] / 1000 for g in groups)
+        workload = (f"uneven batch: 8,192 rWW sims = 16 groups of 512 over nodes {C2_NODES} x durations "
+                    f"{C2_DURATIONS} s divided by {scale:g}, delays 6 m/s (70-mm sphere x 1.3), SC 20%, "
+                    f"w_p = w_p0 + w_p1 map, FP32, one cbnm_run_batch call")
+        for _ in range(opts.warmup):
+            core.run_batch([_copy_args(g) for g in groups])
+        clocks.start()
+        times, launches, h2d, d2h = [], 0, 0, 0
+        for _ in range(opts.steps):
+            gs = [_copy_args(g) for g in groups]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            core.run_batch(gs)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            tm = core.last_timing()
+            launches += tm["kernel_launches"]
+            h2d, d2h = tm["h2d_bytes"], tm["d2h_bytes"]
+        ck = clocks.stop()
+        ms = 1e3 * float(np.mean(times))
+        value = sim_s / (ms / 1e3)
+        e2e = {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "note": "the batch entry point takes host buffers: value is end to end"}
+        # CPU: 2 x threads simulations of every (nodes, duration) group for 2 s, summed per group
+        per_group = []
+        for g in groups:
+            v, el = _oracle_sample(g, 2 * threads, duration_s=2)
+            per_group.append(g[14] * g[16] / 1000 / v)  # extrapolated seconds for the group
+        cpu = {"value": sim_s / sum(per_group), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{2 * threads} sims x 2 s of each group, extrapolated per group to the batch"}
+        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+        extra["scale"] = scale
+    elif opts.config == "c3":
+        nodes, N, dur = 200, 512, 300
+        sc = synthetic.synthetic_sc(nodes, 0.25, 3)
+        rng = np.random.default_rng(33)
+        args = list(synthetic.synthetic_args("rWW", N=N, nodes=nodes, duration_s=dur, seed=3, density=0.25,
+                                             G=rng.uniform(0.001, 10, N), J_N=rng.uniform(0.001, 0.5, N),
+                                             precision="fp32", window_size=30, window_step=5, bold_remove_s=30))
+        args[1] = np.ascontiguousarray(sc.ravel())[None, :]
+        workload = "gradient config: rWW 512 sims, 200 nodes, 300 s, SC 25%, FP32, FC+FCD w30/s5"
+        sim_s = N * dur
+        step, _ = device_runner(args)
+        for _ in range(opts.warmup):
+            step()
+        clocks.start()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        launches = 0
+        for _ in range(opts.steps):
+            launches += step()["kernel_launches"]
+        e1.record(st)
+        torch.cuda.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1) / opts.steps
+        value = sim_s / (ms / 1e3)
+        t0 = time.perf_counter()
+        out = core.run_simulations(*_copy_args(args))
+        e2e_s = time.perf_counter() - t0
+        tm = core.last_timing()
+        e2e = {"value": sim_s / e2e_s, "unit": UNIT, "h2d_bytes_per_step": tm["h2d_bytes"],
+               "d2h_bytes_per_step": tm["d2h_bytes"]}
+        # one adjoint gradient (forward + backward) of the fit loss on --grad-sims simulations
+        from cubnm_b200 import grad
+        gs = opts.grad_sims
+        prob = grad.RWWProblem(sc, nodes, dur, segment_steps=1000)
+        emp = synthetic.synthetic_emp_bold(nodes, dur, 7)
+        efc = torch.from_numpy(utils.calculate_fc(emp)).to(dev)
+        efcd = torch.from_numpy(utils.calculate_fcd(emp, 30, 5)).to(dev)
+        G = torch.tensor(rng.uniform(0.5, 3, gs), dtype=torch.float64, device=dev, requires_grad=True)
+        wp = torch.full((gs, nodes), 1.0, dtype=torch.float64, device=dev, requires_grad=True)
+        jn = torch.full((gs, nodes), 0.15, dtype=torch.float64, device=dev, requires_grad=True)
+        wie = torch.ones((gs, nodes), dtype=torch.float64, device=dev)
+        sig = torch.full((gs, nodes), 0.01, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bold = prob.bold(G, wp, jn, wie, sig)
+        loss = grad.rww_fit_loss(bold, efc, efcd, 30, 30, 5).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        extra["gradient"] = {"sims": gs, "seconds": time.perf_counter() - t0,
+                             "forward_ms": prob.last_forward_ms, "backward_ms": prob.last_backward_ms,
+                             "finite": bool(torch.isfinite(G.grad).all().item())}
+        v, el = _oracle_sample(args, 2 * threads, duration_s=10)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{2 * threads} sims x 10 s of the workload, {el:.1f} s wall"}
+        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+    else:  # c4
+        scale = opts.scale or 30.0
+        dur = max(2, int(round(300 / scale)))
+        N = 2048
+        args = c4_args(N, dur)
+        sim_s = N * dur
+        workload = (f"large sparse network: Wilson-Cowan 1,000 nodes, 2,048 sims, 300 s divided by {scale:g}, "
+                    f"SC 10% (sparse gather), delays 6 m/s, FP32")
+        step, _ = device_runner(args)
+        for _ in range(opts.warmup):
+            step()
+        clocks.start()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        launches = 0
+        for _ in range(opts.steps):
+            launches += step()["kernel_launches"]
+        e1.record(st)
+        torch.cuda.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1) / opts.steps
+        value = sim_s / (ms / 1e3)
+        t0 = time.perf_counter()
+        core.run_simulations(*_copy_args(args))
+        e2e_s = time.perf_counter() - t0
+        tm = core.last_timing()
+        e2e = {"value": sim_s / e2e_s, "unit": UNIT, "h2d_bytes_per_step": tm["h2d_bytes"],
+               "d2h_bytes_per_step": tm["d2h_bytes"]}
+        v, el = _oracle_sample(args, threads, duration_s=1)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{threads} sims x 1 s of the workload, {el:.1f} s wall"}
+        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+        extra["scale"] = scale
+    line = {"metric": f"sims x sim-s per wall-s ({opts.config})", "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": opts.steps, "warmup": opts.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)",
+            "config": {"workload": workload, "name": opts.config}, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roof, "cpu_baseline": cpu, "clocks": ck}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,6 +648,10 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per integrator launch")
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"],
+                    help="c1 (default): the headline workload; c0/c2/c3/c4: the other workloads (one GPU)")
+    ap.add_argument("--scale", type=float, default=None, help="c2 / c4: divide the durations by this")
+    ap.add_argument("--grad-sims", type=int, default=64, help="c3: simulations of the timed adjoint gradient")
     ap.add_argument("--ref-budget", type=float, default=240.0,
                     help="reference arm: seconds the timed CPU steps should take together")
     opts = ap.parse_args()
@@ -388,6 +662,9 @@ def main():
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
     if opts.impl == "reference":
         run_reference(opts, rank, world)
+    elif opts.config != "c1":
+        if rank == 0:
+            run_config(opts)
     else:
         run_ours(opts, rank, world, local_rank)
 

@@ -89,6 +89,14 @@ struct IntegrateArgs {
     int *status;                 // device status word (0 = ok)
     double *bw_scratch;          // two-tile kernel: per-CTA Balloon-Windkessel state (pp_bw_scratch_bytes)
     int pp_grid;                 // two-tile kernel: CTAs launched (the scratch holds this many)
+    // lane kernel (integrate_lanes.cu): groups of 16 simulations sharing SC and delay table
+    const int *ln_groups;        // [ln_n_groups][3 + 16] = SC index, delay table, max delay (1 without delays), simulations
+    int ln_n_groups;
+    int ln_grid;                 // CTAs launched (the ring-buffer and Balloon-Windkessel scratch hold this many)
+    float *ln_params;            // [ln_n_groups][nodes][n_regional][16]  (written by the launcher)
+    float *ln_hist;              // [ln_grid][ln_hist_per_cta]  ring buffers [slot][node][16]
+    long long ln_hist_per_cta;   // floats per CTA: (largest max delay + 1) * nodes * 16
+    double *ln_bw;               // [ln_grid][nodes][4][16]  Balloon-Windkessel state
     // Sparse coupling (per-simulation kernels), ELLPACK by target node: entry q of
     // node j at [q * nodes + j]; ell_k entries per node, zero-weight padding last.
     // One entry = the SC weight packed with the source's offset into the ring
@@ -126,6 +134,10 @@ struct GofArgs {
 cudaError_t launch_integrate_fp64(int model, const IntegrateArgs &a, cudaStream_t st);
 cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStream_t st);  // FP32, one CTA per simulation
+// FP32 with 16 simulations on the lanes (integrate_lanes.cu): delays and/or > 128 nodes.
+bool lanes_supported(int model, int nodes, bool numerical_fic);
+int lanes_rows(int nodes);
+cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st);
 bool fp32_supported(int model, int nodes, bool has_delay);
 // Two-tile tensor-core kernel (integrate_pp.cu): rWW, no delays, <= 128 nodes.
 // Work items: [n_tiles][1 + 64] = SC index, then 32 simulation ids per half (-1 = empty).

@@ -316,7 +316,7 @@ struct Session {
     // run buffers
     DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
-    DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr;
+    DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr, d_ln_groups, d_ln_params, d_ln_hist, d_ln_bw;
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -370,7 +370,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr,
+                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -645,6 +645,17 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         }
         has_delay = *std::max_element(h_max_delay.begin(), h_max_delay.end()) > 0;
     }
+    // FP32 kernels: the tensor-core tiles take shared-SC batches without delays or
+    // numerical FIC at <= 128 nodes; the lane kernel takes delays and larger
+    // networks of the models it implements; everything else in FP32 runs on the
+    // per-simulation kernel.  CBNM_FP32_KERNEL=simt forces the latter.
+    const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
+    const bool force_simt = fp32_kernel && std::string(fp32_kernel) == "simt";
+    const bool num_fic = c.do_fic && c.max_fic_trials > 0;
+    const bool use_tc = c.fp32 && !force_simt && fp32_supported(md.id, n, has_delay) && !num_fic;
+    bool use_lanes = c.fp32 && !force_simt && !use_tc && lanes_supported(md.id, n, num_fic) &&
+                     (has_delay ? *std::max_element(h_max_delay.begin(), h_max_delay.end()) + 1 : 2) * (long long)n <
+                         (1LL << 30);
     if (has_delay) {
         S.d_delay.ensure(sizeof(int) * h_delay.size());
         CK(cudaMemcpyAsync(S.d_delay.p, h_delay.data(), sizeof(int) * h_delay.size(), cudaMemcpyHostToDevice, S.st));
@@ -655,8 +666,11 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         S.d_hist_off.ensure(sizeof(long long) * N);
         CK(cudaMemcpyAsync(S.d_hist_off.p, h_hist_off.data(), sizeof(long long) * N, cudaMemcpyHostToDevice, S.st));
         // FP32 mode keeps FP32 ring buffers, except for the Kuramoto phase (double)
-        if (c.fp32 && !md.osc) S.d_hist_f32.ensure(sizeof(float) * hist_total);
-        else S.d_hist.ensure(sizeof(double) * hist_total);
+        if (c.fp32 && !md.osc) {
+            if (!use_lanes) S.d_hist_f32.ensure(sizeof(float) * hist_total);
+        } else {
+            S.d_hist.ensure(sizeof(double) * hist_total);
+        }
     }
 
     // ---- outputs on the device
@@ -726,12 +740,6 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     ia.n_regional = md.n_regional;
     ia.status = d_status;
     int launches = 0;
-    // The tensor-core tile kernel takes shared-SC batches without delays or
-    // numerical FIC at <= 128 nodes; every other FP32 request runs on the FP32
-    // per-simulation kernel.  CBNM_FP32_KERNEL=simt forces the latter.
-    const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
-    const bool use_tc = c.fp32 && !(fp32_kernel && std::string(fp32_kernel) == "simt") &&
-                        fp32_supported(md.id, n, has_delay) && !(c.do_fic && c.max_fic_trials > 0);
     if (c.fp32) {  // FP32 SC copy (converted once per run)
         std::vector<float> f;
         std::vector<double> tmp;
@@ -771,7 +779,9 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         const std::string mode = cpl ? cpl : "";
         const long long max_hist = has_delay ? (long long)*std::max_element(h_max_delay.begin(), h_max_delay.end()) * n : 0;
         const bool fits = max_hist < (1LL << 30);
-        const bool sparse = fits && (mode == "sparse" || (mode != "dense" && n >= 32 && 2 * kmax <= n));
+        const bool sparse =
+            fits && (use_lanes || mode == "sparse" || (mode != "dense" && n >= 32 && 2 * kmax <= n));
+        if (!fits) use_lanes = false;
         if (sparse) {
             const int K = std::max(kmax, 1);
             const int tabs = has_delay ? (int)(h_delay.size() / nn) : 1;
@@ -858,6 +868,55 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         CK(cudaEventRecord(S.ev[1], S.st));
         if (use_pp) CK(launch_integrate_pp(md.id, ia, S.st, &launches));
         else CK(launch_integrate_fp32(md.id, ia, S.st, &launches));
+    } else if (use_lanes) {
+        // groups of 16 simulations sharing SC and delay table (bnm.cu runs one
+        // CTA per simulation; here one CTA integrates a group)
+        std::vector<int> sc_of(N);
+        if (device_io) {
+            if (h_sc_idx.size() != (size_t)N) {
+                h_sc_idx.resize(N);
+                CK(cudaMemcpy(h_sc_idx.data(), a->sc_indices, sizeof(int) * N, cudaMemcpyDeviceToHost));
+            }
+            sc_of.assign(h_sc_idx.begin(), h_sc_idx.end());
+        } else {
+            sc_of.assign(a->sc_indices, a->sc_indices + N);
+        }
+        std::vector<int> order(N);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return std::make_pair(sc_of[x], h_delay_idx[x]) < std::make_pair(sc_of[y], h_delay_idx[y]);
+        });
+        constexpr int G = 16;
+        std::vector<int> groups;
+        int max_slots = 2;
+        for (size_t i = 0; i < order.size();) {
+            const int sc = sc_of[order[i]], tab = h_delay_idx[order[i]];
+            const int D = has_delay ? std::max(1, h_max_delay[order[i]]) : 1;
+            max_slots = std::max(max_slots, D + 1);
+            groups.push_back(sc);
+            groups.push_back(has_delay ? tab : 0);
+            groups.push_back(D);
+            int cnt = 0;
+            while (cnt < G && i < order.size() && sc_of[order[i]] == sc && h_delay_idx[order[i]] == tab) {
+                groups.push_back(order[i]);
+                ++i;
+                ++cnt;
+            }
+            for (; cnt < G; ++cnt) groups.push_back(-1);
+        }
+        ia.ln_n_groups = (int)(groups.size() / (3 + G));
+        ia.ln_grid = std::min(ia.ln_n_groups, sm_count());
+        S.d_ln_groups.ensure(sizeof(int) * groups.size());
+        CK(cudaMemcpyAsync(S.d_ln_groups.p, groups.data(), sizeof(int) * groups.size(), cudaMemcpyHostToDevice, S.st));
+        ia.ln_groups = S.d_ln_groups.as<int>();
+        ia.ln_params = (float *)S.d_ln_params.ensure(sizeof(float) * (size_t)ia.ln_n_groups * n * md.n_regional * G);
+        ia.ln_hist_per_cta = (long long)max_slots * n * G;
+        ia.ln_hist = (float *)S.d_ln_hist.ensure(sizeof(float) * (size_t)ia.ln_grid * ia.ln_hist_per_cta);
+        ia.ln_bw = (double *)S.d_ln_bw.ensure(sizeof(double) * (size_t)ia.ln_grid * n * 4 * G);
+        CK(cudaStreamSynchronize(S.st));
+        CK(cudaEventRecord(S.ev[1], S.st));
+        CK(launch_integrate_lanes(md.id, ia, S.st));
+        launches += 2;  // parameter layout + integrator
     } else if (c.fp32) {
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));
