@@ -162,6 +162,23 @@ cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();
 
+// Loss of the gradient fit, (1 - r(FC)) + W1(FCD), and dL/dBOLD (fit_loss.cu).
+struct FitLossArgs {
+    int nodes, bold_len, n_vols_remove, n_pairs, n_windows, n_window_pairs;
+    int sim_begin, sim_count, want_grad;
+    const int *w_start, *w_end;  // [n_windows] inclusive volume ranges
+    const double *bold;          // [n_sims][bold_len][nodes]
+    const double *emp_c;         // [n_pairs] empirical FC minus its mean
+    double emp_norm;             // |emp_c|
+    const double *emp_q;         // [n_window_pairs] empirical FCD quantile at each simulated rank
+    double *loss_fc, *loss_fcd;  // [n_sims]
+    double *dbold;               // [n_sims][bold_len][nodes]
+    // scratch of the chunk [sim_count]...
+    double *fc, *wfc, *fcd, *wstat, *stats, *g_fc, *g_fcd, *g_wfc;
+};
+cudaError_t launch_fit_loss(const FitLossArgs &a, cudaStream_t st, int *launches);
+size_t fit_loss_sort_smem(int n_window_pairs);
+
 // Adjoint (reverse-mode) pass of the FP32 rWW integrator + FP64 Balloon-Windkessel
 // model with the noise held fixed (adjoint.cu).  Checkpoints of the state every
 // seg_bw Balloon-Windkessel steps; the backward pass recomputes each segment

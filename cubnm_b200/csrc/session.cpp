@@ -317,6 +317,7 @@ struct Session {
     DBuf d_sc, d_sc_f32, d_sc_idx, d_g, d_r, d_v, d_delay, d_delay_idx, d_max_delay, d_hist_off, d_hist, d_hist_f32;
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
     DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr, d_ln_groups, d_ln_params, d_ln_hist, d_ln_bw;
+    DBuf fl_ec, fl_q, fl_win, fl_scr;  // fit loss
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -370,7 +371,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw,
+                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw, &S.fl_ec, &S.fl_q, &S.fl_win, &S.fl_scr,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -1384,6 +1385,106 @@ int cbnm_adjoint_backward(const cbnm_run_args *a, int segment_steps, const doubl
                           void *scratch, double *grad_global, double *grad_regional) {
     return guarded([&] {
         adjoint_backward_impl(a, segment_steps, dbold, checkpoints, scratch, grad_global, grad_regional);
+    });
+}
+
+// (1 - r(FC)) + W1(FCD) of device BOLD and its gradient (fit_loss.cu).
+static void fit_loss_impl(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove, int window_size,
+                          int window_step, int drop_edges, const double *emp_fc, const double *emp_fcd,
+                          int n_emp_fcd, double *loss_fc, double *loss_fcd, double *dbold) {
+    if (!bold || !emp_fc || !loss_fc || !loss_fcd) throw Err(CBNM_ERR_ARG, "null array");
+    if (n_sims < 1 || nodes < 2 || bold_len < 2 || n_vols_remove < 0 || window_step < 1 || window_size < 0)
+        throw Err(CBNM_ERR_ARG, "invalid sizes");
+    const int corr_len = bold_len - n_vols_remove;
+    if (corr_len < 2) throw Err(CBNM_ERR_CONFIG, "fewer than 2 BOLD volumes for FC");
+    // windows as build_cfg (utils.cpp:21-52)
+    std::vector<int> ws, we;
+    {
+        const int half = window_size / 2;
+        const int first = (drop_edges ? half : 0) + n_vols_remove;
+        const int last = (drop_edges ? corr_len - 1 - half : corr_len - 1) + n_vols_remove;
+        for (int ctr = first; ctr <= last; ctr += window_step) {
+            ws.push_back(std::max(0, ctr - half));
+            we.push_back(std::min(bold_len - 1, ctr + half));
+        }
+    }
+    const int W = (int)ws.size();
+    const int P = nodes * (nodes - 1) / 2, M = W * (W - 1) / 2;
+    if (W > 1024) throw Err(CBNM_ERR_UNSUPPORTED, "at most 1024 dynamic FC windows are supported");
+    if (fit_loss_sort_smem(std::max(1, M)) > 200 * 1024)
+        throw Err(CBNM_ERR_UNSUPPORTED, "too many FCD values for the in-block sort (" + std::to_string(M) + ")");
+    if (M > 0 && (!emp_fcd || n_emp_fcd < 1)) throw Err(CBNM_ERR_ARG, "the FCD term needs the empirical FCD");
+    // empirical FC centred; empirical FCD quantiles at the simulated ranks
+    std::vector<double> ec(emp_fc, emp_fc + P), q(std::max(1, M), 0.0);
+    double em = 0.0;
+    for (double v : ec) em += v;
+    em /= P;
+    double en = 0.0;
+    for (double &v : ec) { v -= em; en += v * v; }
+    en = std::sqrt(en);
+    if (M > 0) {
+        std::vector<double> es(emp_fcd, emp_fcd + n_emp_fcd);
+        std::sort(es.begin(), es.end());
+        for (int i = 0; i < M; ++i) {
+            const long long k = std::min<long long>(n_emp_fcd - 1, (long long)std::floor((i + 0.5) / M * n_emp_fcd));
+            q[i] = es[k];
+        }
+    }
+    Session &S = session();
+    S.fl_ec.ensure(sizeof(double) * P);
+    S.fl_q.ensure(sizeof(double) * q.size());
+    S.fl_win.ensure(sizeof(int) * 2 * std::max(1, W));
+    CK(cudaMemcpyAsync(S.fl_ec.p, ec.data(), sizeof(double) * P, cudaMemcpyHostToDevice, S.st));
+    CK(cudaMemcpyAsync(S.fl_q.p, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, S.st));
+    if (W > 0) {
+        CK(cudaMemcpyAsync(S.fl_win.p, ws.data(), sizeof(int) * W, cudaMemcpyHostToDevice, S.st));
+        CK(cudaMemcpyAsync(S.fl_win.as<int>() + W, we.data(), sizeof(int) * W, cudaMemcpyHostToDevice, S.st));
+    }
+    FitLossArgs f{};
+    f.nodes = nodes; f.bold_len = bold_len; f.n_vols_remove = n_vols_remove; f.n_pairs = P; f.n_windows = W;
+    f.n_window_pairs = M; f.want_grad = dbold != nullptr;
+    f.w_start = S.fl_win.as<int>(); f.w_end = S.fl_win.as<int>() + W;
+    f.bold = bold; f.emp_c = S.fl_ec.as<double>(); f.emp_norm = en; f.emp_q = S.fl_q.as<double>();
+    f.loss_fc = loss_fc; f.loss_fcd = loss_fcd; f.dbold = dbold;
+    // per-simulation scratch, chunked to <= 1 GiB
+    const size_t per = sizeof(double) * ((size_t)2 * P + (size_t)2 * W * P + 2 * (size_t)std::max(1, M) + 2 * (size_t)W +
+                                         (size_t)2 * nodes * (W + 1));
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(n_sims, ((size_t)1 << 30) / per));
+    double *base = (double *)S.fl_scr.ensure(per * chunk);
+    int launches = 0;
+    CK(cudaEventRecord(S.ev[0], S.st));
+    for (int s0 = 0; s0 < n_sims; s0 += chunk) {
+        f.sim_begin = s0;
+        f.sim_count = std::min(chunk, n_sims - s0);
+        const size_t c = (size_t)chunk;
+        double *p = base;
+        f.fc = p; p += c * P;
+        f.g_fc = p; p += c * P;
+        f.wfc = p; p += c * W * P;
+        f.g_wfc = p; p += c * W * P;
+        f.fcd = p; p += c * std::max(1, M);
+        f.g_fcd = p; p += c * std::max(1, M);
+        f.wstat = p; p += c * 2 * W;
+        f.stats = p;
+        CK(launch_fit_loss(f, S.st, &launches));
+    }
+    CK(cudaEventRecord(S.ev[1], S.st));
+    CK(cudaStreamSynchronize(S.st));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]);
+    cbnm_timing tm{};
+    tm.fc_ms = ms;
+    tm.total_ms = ms;
+    tm.kernel_launches = launches;
+    g_last_timing = tm;
+}
+
+int cbnm_fit_loss(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove, int window_size,
+                  int window_step, int drop_edges, const double *emp_fc, const double *emp_fcd, int n_emp_fcd,
+                  double *loss_fc, double *loss_fcd, double *dbold) {
+    return guarded([&] {
+        fit_loss_impl(bold, n_sims, bold_len, nodes, n_vols_remove, window_size, window_step, drop_edges, emp_fc,
+                      emp_fcd, n_emp_fcd, loss_fc, loss_fcd, dbold);
     });
 }
 

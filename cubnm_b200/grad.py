@@ -13,10 +13,13 @@ The forward is the FP32 per-simulation rWW integrator (FP64 Balloon-Windkessel),
 checkpointed every ``segment_steps`` integration steps; the backward recomputes
 each segment from its checkpoint and runs it in reverse on the GPU.
 
-Losses (FP64 torch, differentiable): :func:`fc_tril`, :func:`fcd_tril`,
-:func:`fc_corr_loss` (1 - Pearson r of FC lower triangles) and
-:func:`fcd_wasserstein` (1-D Wasserstein distance of FCD value distributions
-from sorted values), combined by :func:`rww_fit_loss`.
+Loss: :func:`rww_fit_loss` = (1 - Pearson r of FC lower triangles) + the 1-D
+Wasserstein distance of FCD value distributions from sorted values.  On the
+GPU it runs the library's hand-written FP64 kernels for the loss and its
+gradient (``cbnm_fit_loss``); :func:`rww_fit_loss_torch` (built from
+:func:`fc_tril`, :func:`fcd_tril`, :func:`fc_corr_loss`,
+:func:`fcd_wasserstein`) is the torch restatement used on the CPU and as the
+check.
 """
 import ctypes as C
 
@@ -41,6 +44,9 @@ def _declare(L):
     L.cbnm_adjoint_forward.restype = C.c_int
     L.cbnm_adjoint_backward.argtypes = [ap, C.c_int, vp, vp, vp, vp, vp]
     L.cbnm_adjoint_backward.restype = C.c_int
+    L.cbnm_fit_loss.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int,
+                                vp, vp, vp]
+    L.cbnm_fit_loss.restype = C.c_int
     L._adjoint_declared = True
     return L
 
@@ -101,10 +107,44 @@ def fcd_wasserstein(sim_fcd, emp_fcd):
     return (torch.sort(sim_fcd, dim=1).values - q).abs().mean(dim=1)
 
 
-def rww_fit_loss(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges=True):
-    """Per-simulation loss (1 - r(FC)) + W1(FCD) on BOLD [N, T, n]."""
+def rww_fit_loss_torch(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges=True):
+    """Per-simulation loss (1 - r(FC)) + W1(FCD) on BOLD [N, T, n], in torch (FP64
+    autograd): the reference the hand-written kernels are checked against."""
     return (fc_corr_loss(fc_tril(bold, n_vols_remove), emp_fc) +
             fcd_wasserstein(fcd_tril(bold, n_vols_remove, window_size, window_step, drop_edges), emp_fcd))
+
+
+def rww_fit_loss(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges=True):
+    """Per-simulation loss (1 - r(FC)) + W1(FCD) on BOLD [N, T, n] (float64).
+
+    On a CUDA tensor the loss and its gradient come from the library's
+    hand-written kernels (``cbnm_fit_loss``: FC, window FCs, FCD, sort, W1 and the
+    chain rule back to BOLD in one pass); elsewhere from the torch restatement."""
+    if not bold.is_cuda:
+        return rww_fit_loss_torch(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges)
+    return _LOSS.apply(bold, emp_fc, emp_fcd, int(n_vols_remove), int(window_size), int(window_step), bool(drop_edges))
+
+
+def fit_loss_terms(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges=True, grad=False):
+    """The two loss terms (1 - r(FC), W1(FCD)) of BOLD [N, T, n] on the device, and
+    d(sum of both)/dBOLD when ``grad``: (loss_fc [N], loss_fcd [N], dbold or None)."""
+    import torch
+    L = _declare(lib())
+    bold = bold.detach().to(torch.float64).contiguous()
+    N, T, n = bold.shape
+    efc = np.ascontiguousarray(np.asarray(emp_fc.detach().cpu() if hasattr(emp_fc, "detach") else emp_fc,
+                                          dtype=np.float64))
+    efcd = np.ascontiguousarray(np.asarray(emp_fcd.detach().cpu() if hasattr(emp_fcd, "detach") else emp_fcd,
+                                           dtype=np.float64))
+    lf = torch.empty(N, dtype=torch.float64, device=bold.device)
+    ld = torch.empty(N, dtype=torch.float64, device=bold.device)
+    db = torch.empty_like(bold) if grad else None
+    torch.cuda.synchronize(bold.device)  # the library works on its own stream
+    dp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    check(L.cbnm_fit_loss(_ptr(bold), N, T, n, int(n_vols_remove), int(window_size), int(window_step),
+                          int(bool(drop_edges)), dp(efc), dp(efcd), int(efcd.size), _ptr(lf), _ptr(ld),
+                          _ptr(db) if db is not None else None))
+    return lf, ld, db
 
 
 class RWWProblem:
@@ -229,12 +269,43 @@ def _autograd_function():
 
 class _Lazy:
     fn = None
+    make = staticmethod(_autograd_function)
 
     @classmethod
     def apply(cls, *args):
         if cls.fn is None:
-            cls.fn = _autograd_function()
+            cls.fn = cls.make()
         return cls.fn.apply(*args)
 
 
-_BOLD = _Lazy
+def _loss_function():
+    import torch
+
+    class Loss(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges):
+            lf, ld, db = fit_loss_terms(bold, emp_fc, emp_fcd, n_vols_remove, window_size, window_step, drop_edges,
+                                        grad=ctx.needs_input_grad[0])
+            ctx.save_for_backward(db if db is not None else torch.empty(0))
+            return (lf + ld).to(bold.dtype)
+
+        @staticmethod
+        def backward(ctx, go):
+            (db,) = ctx.saved_tensors
+            return (go.to(db.dtype)[:, None, None] * db), None, None, None, None, None, None
+
+    return Loss
+
+
+class _LazyBOLD(_Lazy):
+    fn = None
+    make = staticmethod(_autograd_function)
+
+
+class _LazyLoss(_Lazy):
+    fn = None
+    make = staticmethod(_loss_function)
+
+
+_BOLD = _LazyBOLD
+_LOSS = _LazyLoss

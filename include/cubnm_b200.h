@@ -216,6 +216,24 @@ int cbnm_adjoint_backward(const cbnm_run_args *args, int segment_steps, const do
                           const void *checkpoints, void *scratch, double *grad_global,
                           double *grad_regional);
 
+/* Loss of the gradient fit and its gradient with respect to BOLD, for simulated
+ * BOLD in device memory.  No counterpart in the reference, whose optimisers score
+ * simulations by GOF terms without derivatives (src/cubnm/sim/base.py:1084-1207,
+ * src/cubnm/optimize.py); the terms are those scores made differentiable:
+ *   loss_fc[s]  = 1 - Pearson r(FC lower triangle of s, emp_fc)
+ *   loss_fcd[s] = W1 between the FCD values of s and emp_fcd: mean over the m
+ *                 sorted simulated values of |sorted_i - Q_emp((i + 1/2) / m)|,
+ *                 Q_emp(p) = sorted emp_fcd[floor(p n_emp_fcd)]  (0 with < 2 windows)
+ * FC / FCD as run_simulations computes them (volumes [n_vols_remove, bold_len),
+ * windows of window_size / window_step / drop_edges, src/ext/utils.cpp:21-52).
+ *   bold   [n_sims][bold_len][nodes] device; emp_fc [n_pairs] and emp_fcd host;
+ *   loss_fc, loss_fcd [n_sims] device; dbold [n_sims][bold_len][nodes] device =
+ *   d(loss_fc + loss_fcd)/dBOLD per simulation, or NULL for the loss only.
+ * FP64 throughout; the call returns when the results are written. */
+int cbnm_fit_loss(const double *bold, int n_sims, int bold_len, int nodes, int n_vols_remove, int window_size,
+                  int window_step, int drop_edges, const double *emp_fc, const double *emp_fcd, int n_emp_fcd,
+                  double *loss_fc, double *loss_fcd, double *dbold);
+
 /* FC and FCD of simulated BOLD already in device memory, allocating no device
  * memory.  No counterpart in the reference: there, FC and FCD are computed only
  * inside run_simulations (src/ext/bnm.cu:809-942).  It is for callers that
