@@ -96,7 +96,8 @@ struct IntegrateArgs {
     float *ln_params;            // [ln_n_groups][nodes][n_regional][16]  (written by the launcher)
     float *ln_hist;              // [ln_grid][ln_hist_per_cta]  ring buffers [slot][node][16]
     long long ln_hist_per_cta;   // floats per CTA: (largest max delay + 1) * nodes * 16
-    double *ln_bw;               // [ln_grid][nodes][4][16]  Balloon-Windkessel state
+    double *ln_bw;               // [ln_grid][nodes][4 or 8][16]  Balloon-Windkessel state (+ its tangent)
+    double *tan_bold;            // non-null: the lane kernel also integrates d/dG, dBOLD/dG here [n_sims][bold_len][nodes]
     // Sparse coupling (per-simulation kernels), ELLPACK by target node: entry q of
     // node j at [q * nodes + j]; ell_k entries per node, zero-weight padding last.
     // One entry = the SC weight packed with the source's offset into the ring
@@ -136,6 +137,7 @@ cudaError_t launch_integrate_fp32(int model, const IntegrateArgs &a, cudaStream_
 cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStream_t st);  // FP32, one CTA per simulation
 // FP32 with 16 simulations on the lanes (integrate_lanes.cu): delays and/or > 128 nodes.
 bool lanes_supported(int model, int nodes, bool numerical_fic);
+bool lanes_tangent_supported(int model);
 int lanes_rows(int nodes);
 cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st);
 bool fp32_supported(int model, int nodes, bool has_delay);

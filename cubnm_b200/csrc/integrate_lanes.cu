@@ -1,225 +1,7 @@
-// FP32 integrator with the simulations on the lanes, for the networks the
-// tensor-core tiles do not take: conduction delays (any node count) and more than
-// 128 nodes.  The time loop is the reference's (src/ext/bnm.cu:117-505); the
-// delayed coupling is bnm.cu:48-77 with the ring-buffer index of bnm.cu:28-46.
-//
-// The per-simulation kernel (integrate_sim.cuh, the reference's one CTA per
-// simulation and one thread per node) gathers x_k(t - d_kj) from the
-// simulation's own ring buffer: each 4-byte value costs a 32-byte sector, and
-// every simulation re-reads the SC / delay entries.  Here 16 simulations that
-// share one SC and one delay table are integrated together, simulation s on
-// lane s of a half-warp:
-//
-//  * thread (node row r = tid / 16, simulation s = tid % 16) updates nodes
-//    j = r, r + NT/16, r + 2 NT/16, ... (MN of them) of simulation s, state in
-//    registers;
-//  * the ring buffer of the group is [slot][node][16 simulations] (FP32), so the
-//    16 lanes that need x_k(t - d_kj) of their own simulation read 64 contiguous
-//    bytes, and the packed ELLPACK entry {d n + k, weight} of (j, q) is the same
-//    address for the half-warp;
-//  * the buffer has max_delay + 1 slots: step t reads slots buff + d (d >= 1) and
-//    writes slot buff, which no read of step t touches, so one barrier per step
-//    orders the writes of step t before the reads of step t + 1.  Without delays
-//    the coupling reads the previous step (d = 1, two slots);
-//  * parameters are an FP32 copy laid out [node][param][16]; the FP64
-//    Balloon-Windkessel state is in global memory [node][4][16] (updated once per
-//    bw step, series form of tc_common.cuh); noise is shared by all simulations.
-// The coupling sum runs over the nonzeros in ascending source order from zero, as
-// the per-simulation kernel's, so the node states are the same as that kernel's.
-#include <algorithm>
-#include "engine.h"
-#include "integrate_sim.cuh"
-#include "tc_common.cuh"
+// FP32 lane kernel: the forward integrator (see lanes.cuh for the design).
+#include "lanes.cuh"
 
 namespace cbnm {
-namespace {
-
-constexpr int LN_SIMS = 16;   // simulations per group (a half-warp)
-
-// States of node j of simulation sim after a sample step: the time series, or
-// the running sums of the kept samples.  Out of line: it runs once per sample.
-template <int NS>
-__device__ __noinline__ void lanes_states_out(const IntegrateArgs &a, const float *st, int sim, int j, int states_i) {
-    const int n = a.nodes;
-    const size_t ext = a.states_ts ? (size_t)n * a.states_len : (size_t)n;
-    for (int v = 0; v < NS; ++v) {
-        if (a.states_ts) {
-            if (states_i < a.states_len) a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = (double)st[v];
-        } else if (states_i >= a.n_states_samples_remove) {
-            a.states[((size_t)v * a.n_sims + sim) * ext + j] += (double)st[v];
-        }
-    }
-}
-
-template <class M, int NT, int MN, bool DELAY>
-__global__ void __launch_bounds__(NT, 1) k_integrate_lanes(const __grid_constant__ IntegrateArgs a) {
-    static_assert(!M::OSC, "phase models run on the per-simulation kernel (numerical FIC too, by the host)");
-    constexpr int ROW = NT / LN_SIMS;  // node rows per CTA
-    using R = float;
-    const int tid = threadIdx.x;
-    const int s = tid & (LN_SIMS - 1);
-    const int r0 = tid >> 4;
-    const int n = a.nodes;
-    const int EK = a.ell_k;
-    const size_t rstride = (size_t)a.n_sims * n;
-    const size_t ext = a.states_ts ? (size_t)n * a.states_len : (size_t)n;
-    const BW64 &bw = a.bwf;
-    float *hist = a.ln_hist + (size_t)blockIdx.x * a.ln_hist_per_cta;
-    double *bws = a.ln_bw + (size_t)blockIdx.x * n * 4 * LN_SIMS;
-
-    for (int gi = blockIdx.x; gi < a.ln_n_groups; gi += gridDim.x) {
-        const int *gd = a.ln_groups + (size_t)gi * (3 + LN_SIMS);
-        const int sc_i = gd[0], table = gd[1], D = gd[2];   // D: the group's largest delay (1 without delays)
-        const int sim = gd[3 + s];
-        const bool live = sim >= 0;
-        const float *par = a.ln_params + (size_t)gi * n * M::NR * LN_SIMS;
-        const int2 *ell = a.ell_pk32 + (size_t)(sc_i * a.ell_tables + table) * EK * n;
-        R g[M::NG], iv[M::NI], st[MN][M::NS];
-#pragma unroll
-        for (int i = 0; i < M::NG; ++i) g[i] = live ? (R)a.gparams[(size_t)i * a.n_sims + sim] : R(0);
-#pragma unroll
-        for (int i = 0; i < M::NI; ++i) iv[i] = R(0);
-        const int slots = D + 1, hw = slots * n;
-#pragma unroll
-        for (int m = 0; m < MN; ++m) {
-            const int j = r0 + ROW * m;
-#pragma unroll
-            for (int v = 0; v < M::NS; ++v) st[m][v] = R(0);
-            if (j >= n) continue;
-            R r[M::NR];
-#pragma unroll
-            for (int q = 0; q < M::NR; ++q) r[q] = par[((size_t)j * M::NR + q) * LN_SIMS + s];
-            M::init(st[m], iv, g, r);
-            for (int b = 0; b < slots; ++b) hist[((size_t)b * n + j) * LN_SIMS + s] = st[m][M::CONN];
-            double *bj = bws + (size_t)j * 4 * LN_SIMS + s;
-            bj[0] = 0.0;
-            bj[LN_SIMS] = 1.0;
-            bj[2 * LN_SIMS] = 1.0;
-            bj[3 * LN_SIMS] = 1.0;
-            if (live && a.ext_out && !a.states_ts)
-                for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] = 0.0;
-        }
-        __syncthreads();
-
-        int buff = D, bold_i = 0, states_i = 0, repeat = 0;
-        int shj[MN];
-#pragma unroll
-        for (int m = 0; m < MN; ++m) shj[m] = (r0 + ROW * m < n) ? a.sh_nodes[r0 + ROW * m] : 0;
-        double *bold = a.bold + (size_t)(live ? sim : 0) * a.bold_len * n;
-        for (int bw_i = 0; bw_i < a.bw_it; ++bw_i) {
-            const int sh_ts = a.sh_ts[(bw_i % a.noise_bw_it) + repeat * a.noise_bw_it];
-            const bool sample = a.ext_out && (bw_i + 1) % a.states_sampling_iters == 0;  // bnm.cpp:337-355
-            for (int inner = 0; inner < a.inner_it; ++inner) {
-                const int hbase = buff * n;
-                const bool out_now = sample && live && inner == a.inner_it - 1;
-#pragma unroll
-                for (int m = 0; m < MN; ++m) {
-                    const int j = r0 + ROW * m;
-                    if (j >= n) continue;
-                    // coupling: sum over the nonzeros of column j of SC[k][j] x_k(t - d_kj)
-                    const int2 *pk = ell + j;
-                    R in = R(0);
-#pragma unroll 4
-                    for (int q = 0; q < EK; ++q) {
-                        const int2 e = __ldg(pk + (size_t)q * n);
-                        int h = hbase + e.x + (DELAY ? 0 : n);
-                        if (h >= hw) h -= hw;
-                        in += __int_as_float(e.y) * hist[(size_t)h * LN_SIMS + s];
-                    }
-                    const long long ni = ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
-                    const R n0 = __ldg(a.noise_f32 + ni);
-                    const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
-                    R r[M::NR];
-#pragma unroll
-                    for (int q = 0; q < M::NR; ++q) r[q] = __ldg(par + ((size_t)j * M::NR + q) * LN_SIMS + s);
-                    M::step(st[m], iv, g, r, in, n0, n1, a.K);
-                    if (out_now) lanes_states_out<M::NS>(a, st[m], sim, j, states_i);
-                }
-#pragma unroll
-                for (int m = 0; m < MN; ++m) {
-                    const int j = r0 + ROW * m;
-                    if (j < n) hist[((size_t)hbase + j) * LN_SIMS + s] = st[m][M::CONN];
-                }
-                __syncthreads();  // this step's slot is written before the next step reads it
-                buff = buff ? buff - 1 : D;
-            }
-            // Balloon-Windkessel (bw.cu:4-15), BOLD at TR (bnm.cpp:316-335)
-            const bool tr = (bw_i + 1) % a.bold_tr_iters == 0;
-#pragma unroll
-            for (int m = 0; m < MN; ++m) {
-                const int j = r0 + ROW * m;
-                if (j >= n || !live) continue;
-                double *bj = bws + (size_t)j * 4 * LN_SIMS + s;
-                double x = bj[0], f = bj[LN_SIMS], nu = bj[2 * LN_SIMS], q = bj[3 * LN_SIMS];
-                bw_step64(x, f, nu, q, (double)st[m][M::BOLDV], bw);
-                bj[0] = x;
-                bj[LN_SIMS] = f;
-                bj[2 * LN_SIMS] = nu;
-                bj[3 * LN_SIMS] = q;
-                if (tr && bold_i < a.bold_len)  // no slot for a sample past bold_len
-                    bold[(size_t)bold_i * n + j] = bw.V0k1 * (1 - q) + bw.V0k2 * (1 - q / nu) + bw.V0k3 * (1 - nu);
-            }
-            if (tr) bold_i++;
-            if (sample) states_i++;
-            if ((bw_i + 1) % a.noise_bw_it == 0 && bw_i + 1 < a.bw_it) {
-                repeat++;
-#pragma unroll
-                for (int m = 0; m < MN; ++m)
-                    if (r0 + ROW * m < n) shj[m] = a.sh_nodes[(size_t)repeat * n + r0 + ROW * m];
-            }
-        }
-        if (live && a.ext_out && !a.states_ts) {
-            const int pts = states_i - a.n_states_samples_remove;
-#pragma unroll
-            for (int m = 0; m < MN; ++m) {
-                const int j = r0 + ROW * m;
-                if (j >= n) continue;
-                for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] /= pts;
-            }
-        }
-        __syncthreads();  // the next group reuses the ring buffer and the Balloon-Windkessel scratch
-    }
-}
-
-// Parameters of every group in the lane layout: out[g][j][q][s] = (float)
-// regional[q][sim(g, s)][j] (zero for empty lanes).
-__global__ void k_lanes_params(const IntegrateArgs a, int nr, float *out) {
-    const int g = blockIdx.x;
-    const int n = a.nodes;
-    const int *gd = a.ln_groups + (size_t)g * (3 + LN_SIMS);
-    const size_t rstride = (size_t)a.n_sims * n;
-    for (int e = threadIdx.x; e < n * nr * LN_SIMS; e += blockDim.x) {
-        const int s = e % LN_SIMS, q = (e / LN_SIMS) % nr, j = e / (LN_SIMS * nr);
-        const int sim = gd[3 + s];
-        out[(size_t)g * n * nr * LN_SIMS + e] = sim >= 0 ? (float)a.rparams[q * rstride + (size_t)sim * n + j] : 0.0f;
-    }
-}
-
-template <class M, int NT, int MN>
-cudaError_t launch_lanes_mn(const IntegrateArgs &a, cudaStream_t st) {
-    const int grid = std::min(a.ln_n_groups, a.ln_grid);
-    if (a.has_delay) k_integrate_lanes<M, NT, MN, true><<<grid, NT, 0, st>>>(a);
-    else k_integrate_lanes<M, NT, MN, false><<<grid, NT, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
-template <class M>
-cudaError_t launch_lanes_model(const IntegrateArgs &a, cudaStream_t st) {
-    k_lanes_params<<<a.ln_n_groups, 256, 0, st>>>(a, M::NR, a.ln_params);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const int mn = lanes_rows(a.nodes);
-    switch (mn) {
-        case 1: return launch_lanes_mn<M, 1024, 1>(a, st);
-        case 2: return launch_lanes_mn<M, 1024, 2>(a, st);
-        case 4: return launch_lanes_mn<M, 1024, 4>(a, st);
-        case 8: return launch_lanes_mn<M, 1024, 8>(a, st);
-        case 16: return launch_lanes_mn<M, 1024, 16>(a, st);
-    }
-    return cudaErrorInvalidValue;
-}
-
-}  // namespace
 
 // Node rows per thread (a power of two) for a node count: 64 nodes per row.
 int lanes_rows(int nodes) {
@@ -228,18 +10,23 @@ int lanes_rows(int nodes) {
     return mn;
 }
 
+bool lanes_tangent_supported(int model) { return model == MODEL_RWW || model == MODEL_WC; }
+
 bool lanes_supported(int model, int nodes, bool numerical_fic) {
     if (nodes < 1 || nodes > 16 * 64 || numerical_fic) return false;
     if (model == MODEL_JR) return lanes_rows(nodes) <= 4;  // 8 state variables a node in registers
     return model == MODEL_RWW || model == MODEL_WC || model == MODEL_RWWEX;
 }
 
+cudaError_t launch_integrate_lanes_tan(int model, const IntegrateArgs &a, cudaStream_t st);  // integrate_lanes_tan.cu
+
 cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st) {
+    if (a.tan_bold) return launch_integrate_lanes_tan(model, a, st);
     switch (model) {
-        case MODEL_RWW: return launch_lanes_model<RWWm<float>>(a, st);
-        case MODEL_WC: return launch_lanes_model<WCm<float>>(a, st);
-        case MODEL_JR: return launch_lanes_model<JRm<float>>(a, st);
-        case MODEL_RWWEX: return launch_lanes_model<RWWExm<float>>(a, st);
+        case MODEL_RWW: return lanes::launch_model<RWWm<float>, false>(a, st);
+        case MODEL_WC: return lanes::launch_model<WCm<float>, false>(a, st);
+        case MODEL_JR: return lanes::launch_model<JRm<float>, false>(a, st);
+        case MODEL_RWWEX: return lanes::launch_model<RWWExm<float>, false>(a, st);
     }
     return cudaErrorNotSupported;
 }

@@ -526,7 +526,9 @@ static std::vector<int> pair_tiles(const std::vector<int> &tiles, int n_tiles, i
     return out;
 }
 
-static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io) {
+// tan_bold (device, [N][bold_len][nodes]) non-null: also integrate the tangent along
+// G and write dBOLD/dG there (lane kernel, FP32 precision, rWW or WC).
+static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io, double *tan_bold = nullptr) {
     const double t_begin = now_s();
     check_args(a);
     if (!o || !o->sim_bold) throw Err(CBNM_ERR_ARG, "null output arrays");
@@ -653,8 +655,11 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
     const bool force_simt = fp32_kernel && std::string(fp32_kernel) == "simt";
     const bool num_fic = c.do_fic && c.max_fic_trials > 0;
-    const bool use_tc = c.fp32 && !force_simt && fp32_supported(md.id, n, has_delay) && !num_fic;
-    bool use_lanes = c.fp32 && !force_simt && !use_tc && lanes_supported(md.id, n, num_fic) &&
+    if (tan_bold && (!c.fp32 || !lanes_tangent_supported(md.id) || num_fic || !lanes_supported(md.id, n, num_fic)))
+        throw Err(CBNM_ERR_UNSUPPORTED, "the G tangent needs precision fp32, model rWW or WC, at most 1024 nodes and "
+                                        "no numerical FIC");
+    const bool use_tc = !tan_bold && c.fp32 && !force_simt && fp32_supported(md.id, n, has_delay) && !num_fic;
+    bool use_lanes = c.fp32 && (!force_simt || tan_bold) && !use_tc && lanes_supported(md.id, n, num_fic) &&
                      (has_delay ? *std::max_element(h_max_delay.begin(), h_max_delay.end()) + 1 : 2) * (long long)n <
                          (1LL << 30);
     if (has_delay) {
@@ -911,9 +916,10 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         CK(cudaMemcpyAsync(S.d_ln_groups.p, groups.data(), sizeof(int) * groups.size(), cudaMemcpyHostToDevice, S.st));
         ia.ln_groups = S.d_ln_groups.as<int>();
         ia.ln_params = (float *)S.d_ln_params.ensure(sizeof(float) * (size_t)ia.ln_n_groups * n * md.n_regional * G);
-        ia.ln_hist_per_cta = (long long)max_slots * n * G;
+        ia.ln_hist_per_cta = (long long)max_slots * n * G * (tan_bold ? 2 : 1);  // (x, dx/dG) pairs with the tangent
+        ia.tan_bold = tan_bold;
         ia.ln_hist = (float *)S.d_ln_hist.ensure(sizeof(float) * (size_t)ia.ln_grid * ia.ln_hist_per_cta);
-        ia.ln_bw = (double *)S.d_ln_bw.ensure(sizeof(double) * (size_t)ia.ln_grid * n * 4 * G);
+        ia.ln_bw = (double *)S.d_ln_bw.ensure(sizeof(double) * (size_t)ia.ln_grid * n * (tan_bold ? 8 : 4) * G);
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));
         CK(launch_integrate_lanes(md.id, ia, S.st));
@@ -1284,6 +1290,13 @@ int cbnm_run_simulations(const cbnm_run_args *a, cbnm_outputs *o) {
 
 int cbnm_run_simulations_device(const cbnm_run_args *a, cbnm_outputs *o) {
     return guarded([&] { run_impl(nullptr, a, o, true); });
+}
+
+int cbnm_run_tangent_device(const cbnm_run_args *a, cbnm_outputs *o, double *dbold_dG) {
+    return guarded([&] {
+        if (!dbold_dG) throw Err(CBNM_ERR_ARG, "null dBOLD/dG output");
+        run_impl(nullptr, a, o, true, dbold_dG);
+    });
 }
 
 // Groups run concurrently, each worker on its own session (stream, buffers, noise

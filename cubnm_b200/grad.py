@@ -309,3 +309,47 @@ class _LazyLoss(_Lazy):
 
 _BOLD = _LazyBOLD
 _LOSS = _LazyLoss
+
+
+def bold_and_dG(args, device="cuda:0"):
+    """BOLD and dBOLD/dG of a batch given by the reference's 22 run_simulations
+    arguments (host arrays; precision "fp32", model rWW or WC, delays allowed):
+    both [N, bold_len, nodes] float64 torch tensors on ``device``.
+
+    The derivative comes from the tangent-linear integrator (forward mode along
+    each simulation's G, noise held fixed), so dL/dG of any loss on BOLD is
+    ``(dL/dBOLD * dBOLD/dG).sum((1, 2))``, e.g. with the loss kernels::
+
+        bold, dG = bold_and_dG(args)
+        lf, ld, db = fit_loss_terms(bold, emp_fc, emp_fcd, remove, ws, step, grad=True)
+        dL_dG = (db * dG).sum((1, 2))
+    """
+    import torch
+    dev = torch.device(device)
+    L = lib()
+    L.cbnm_run_tangent_device.argtypes = [C.POINTER(_abi.RunArgs), C.POINTER(_abi.Outputs), C.c_void_p]
+    L.cbnm_run_tangent_device.restype = C.c_int
+    prep = _abi.Prepared(*args)
+    sizes = _abi.Sizes()
+    check(L.cbnm_query_sizes(C.byref(prep.args), C.byref(sizes)))
+    N, n = int(args[14]), int(args[15])
+    t = lambda x, dt=torch.float64: torch.from_numpy(np.ascontiguousarray(x)).to(dev, dt)  # noqa: E731
+    keep = {"sc": t(args[1]), "sc_idx": t(np.asarray(args[2], np.int32), torch.int32), "dist": t(args[3]),
+            "g": t(args[4]), "r": t(args[5]), "v": t(args[6])}
+    bold = torch.empty((N, sizes.bold_len, n), dtype=torch.float64, device=dev)
+    dG = torch.zeros_like(bold)
+    fc = torch.empty((N, max(1, sizes.n_pairs)), dtype=torch.float64, device=dev)
+    fcd = torch.empty((N, max(1, sizes.n_window_pairs)), dtype=torch.float64, device=dev)
+    states = torch.empty((sizes.n_state_vars, N, n * (sizes.states_len if args[9] else 1)), dtype=torch.float64,
+                         device=dev)
+    gb = torch.empty((max(1, sizes.n_global_out_bool), N), dtype=torch.uint8, device=dev)
+    gi = torch.empty((max(1, sizes.n_global_out_int), N), dtype=torch.int32, device=dev)
+    dp = lambda x: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+    a = prep.args
+    a.sc, a.sc_dist, a.global_params, a.regional_params, a.v_list = (dp(keep[k]) for k in ("sc", "dist", "g", "r", "v"))
+    a.sc_indices = C.cast(C.c_void_p(keep["sc_idx"].data_ptr()), C.POINTER(C.c_int32))
+    out = _abi.Outputs(dp(bold), dp(fc), dp(fcd), dp(states), C.cast(C.c_void_p(gb.data_ptr()), C.POINTER(C.c_uint8)),
+                       C.cast(C.c_void_p(gi.data_ptr()), C.POINTER(C.c_int32)), None, None, None, 0.0, 0.0)
+    torch.cuda.synchronize(dev)
+    check(L.cbnm_run_tangent_device(C.byref(a), C.byref(out), _ptr(dG)))
+    return bold, dG

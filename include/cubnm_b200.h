@@ -147,6 +147,20 @@ int cbnm_run_simulations(const cbnm_run_args *args, cbnm_outputs *out);
  * No reference counterpart: it is the device-resident form of core.cpp:194-493. */
 int cbnm_run_simulations_device(const cbnm_run_args *args, cbnm_outputs *out);
 
+/* cbnm_run_simulations_device plus the derivative of BOLD with respect to each
+ * simulation's global coupling G, integrated alongside (forward mode: the
+ * tangent of the node state, of the delayed coupling through the ring buffer and
+ * of the FP64 Balloon-Windkessel state; the noise held fixed).  No counterpart
+ * in the reference, which has no derivatives (src/cubnm/optimize.py fits by
+ * grid / CMA-ES); it differentiates the reference's time loop
+ * (src/ext/bnm.cu:117-505, models/wc.cpp:51-80, models/rww.cpp:194-232).
+ * dL/dG of a loss on BOLD is then sum(dL/dBOLD * dBOLD/dG) per simulation.
+ * Forward mode needs no checkpoints, so it serves delayed networks, whose
+ * reverse pass would have to store D steps of ring buffer per checkpoint.
+ * Scope: precision "fp32", models "rWW" and "WC", <= 1024 nodes, no numerical FIC.
+ *   dbold_dG [n_sims][bold_len][nodes] (device), same layout as sim_bold. */
+int cbnm_run_tangent_device(const cbnm_run_args *args, cbnm_outputs *out, double *dbold_dG);
+
 /* Several independent runs ("groups": each a full cbnm_run_simulations call with
  * HOST buffers, possibly of different models, node counts, durations, delays and
  * precisions) executed concurrently.  No counterpart in the reference, whose

@@ -128,3 +128,52 @@ def test_gradients_match_torch_fp64_autograd():
         ref = ref.numpy()
         adj = adj.cpu().numpy()
         assert np.abs(ref - adj).max() <= REL_TOL * np.abs(ref).max() + 1e-10, (name, ref, adj)
+
+
+# ---- G gradients by the tangent-linear integrator (cbnm_run_tangent_device)
+
+def _delayed_args(model, N, nodes, duration_s, seed, precision, G):
+    args = list(cases.synthetic_args(model, N=N, nodes=nodes, duration_s=duration_s, seed=seed, density=0.3, G=G,
+                                     precision=precision, window_size=4, window_step=1, bold_remove_s=1))
+    if model == "WC":
+        reg = args[5].reshape(8, N, nodes)
+        reg[6] = reg[7] = 0.01   # noise as the large-network workload
+    args[3] = np.ascontiguousarray(cases.synthetic_lengths(nodes, seed).ravel())
+    args[6] = np.full(N, 6.0)
+    args[11] = True
+    return args
+
+
+@pytest.mark.parametrize("model,G", [("WC", [0.4, 1.2, 2.5]), ("rWW", [0.5, 1.5, 3.0])])
+def test_tangent_dG_matches_fp64_finite_differences(model, G):
+    """dL/dG of L = sum(w * BOLD) (fixed random weights) and of the fit loss, from
+    dBOLD/dG of the tangent integrator (FP32 state, delays, 6 m/s), against central
+    differences of the FP64 path.  The tangent run's BOLD is the plain FP32 run's."""
+    import torch
+    from cubnm_b200 import core, grad, utils
+    N, nodes, dur = 3, 24, 5
+    G = np.array(G)
+    bold, dG = grad.bold_and_dG(_delayed_args(model, N, nodes, dur, 11, "fp32", G))
+    plain = core.run_simulations(*_delayed_args(model, N, nodes, dur, 11, "fp32", G))["sim_bold"]
+    np.testing.assert_array_equal(bold.cpu().numpy().reshape(N, -1), plain)
+    w = np.random.default_rng(2).standard_normal(bold.shape[1:])
+    tan = (dG.cpu().numpy() * w).sum(axis=(1, 2))
+    emp = cases.synthetic_emp_bold(nodes, dur, 3)
+    efc, efcd = utils.calculate_fc(emp), utils.calculate_fcd(emp, 4, 1)
+    lf, ld, db = grad.fit_loss_terms(bold, efc, efcd, 1, 4, 1, True, grad=True)
+    tan_fit = (db * dG).sum(dim=(1, 2)).cpu().numpy()
+
+    def losses(Gv):
+        o = core.run_simulations(*_delayed_args(model, N, nodes, dur, 11, "fp64", Gv))
+        b = o["sim_bold"].reshape(N, -1, nodes)
+        bt = torch.tensor(b, dtype=torch.float64)
+        fit = grad.rww_fit_loss_torch(bt, torch.tensor(efc), torch.tensor(efcd), 1, 4, 1).numpy()
+        return (b * w).sum(axis=(1, 2)), fit
+
+    h = 1e-4 * np.maximum(1.0, G)
+    (lp, fp), (lm, fm) = losses(G + h), losses(G - h)
+    fd, fd_fit = (lp - lm) / (2 * h), (fp - fm) / (2 * h)
+    rel = np.abs(tan - fd) / np.abs(fd).max()
+    rel_fit = np.abs(tan_fit - fd_fit) / np.abs(fd_fit).max()
+    assert rel.max() < 1e-2, (tan, fd, rel)
+    assert rel_fit.max() < 2e-2, (tan_fit, fd_fit, rel_fit)
