@@ -76,4 +76,17 @@ def reset():
     check(lib().cbnm_reset())
 
 
+def last_integrator():
+    """Which integrator the last run on this thread used: "fp64", or for precision
+    "fp32" one of "tc2", "tc1", "lanes", "lanes512", "simt"."""
+    f = lib().cbnm_last_integrator
+    f.restype = C.c_char_p
+    return f().decode()
+
+
+def tune_reset():
+    """Forgets the autotuner's choices (model_config "autotune" = "1")."""
+    check(lib().cbnm_tune_reset())
+
+
 init()

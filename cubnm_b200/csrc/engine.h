@@ -93,6 +93,7 @@ struct IntegrateArgs {
     const int *ln_groups;        // [ln_n_groups][3 + 16] = SC index, delay table, max delay (1 without delays), simulations
     int ln_n_groups;
     int ln_grid;                 // CTAs launched (the ring-buffer and Balloon-Windkessel scratch hold this many)
+    int ln_threads;              // 1024 (64 node rows a CTA, one CTA an SM) or 512 (32 rows, two an SM; <= 128 nodes)
     float *ln_params;            // [ln_n_groups][nodes][n_regional][16]  (written by the launcher)
     float *ln_hist;              // [ln_grid][ln_hist_per_cta]  ring buffers [slot][node][16]
     long long ln_hist_per_cta;   // floats per CTA: (largest max delay + 1) * nodes * 16
@@ -138,7 +139,7 @@ cudaError_t launch_integrate_simt32(int model, const IntegrateArgs &a, cudaStrea
 // FP32 with 16 simulations on the lanes (integrate_lanes.cu): delays and/or > 128 nodes.
 bool lanes_supported(int model, int nodes, bool numerical_fic);
 bool lanes_tangent_supported(int model);
-int lanes_rows(int nodes);
+int lanes_rows(int nodes, int threads);
 cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st);
 bool fp32_supported(int model, int nodes, bool has_delay);
 // Two-tile tensor-core kernel (integrate_pp.cu): rWW, no delays, <= 128 nodes.

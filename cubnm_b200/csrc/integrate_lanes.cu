@@ -3,10 +3,10 @@
 
 namespace cbnm {
 
-// Node rows per thread (a power of two) for a node count: 64 nodes per row.
-int lanes_rows(int nodes) {
+// Node rows per thread (a power of two) for a node count: threads / 16 nodes per row.
+int lanes_rows(int nodes, int threads) {
     int mn = 1;
-    while (mn * 64 < nodes) mn *= 2;
+    while (mn * (threads / 16) < nodes) mn *= 2;
     return mn;
 }
 
@@ -14,7 +14,7 @@ bool lanes_tangent_supported(int model) { return model == MODEL_RWW || model == 
 
 bool lanes_supported(int model, int nodes, bool numerical_fic) {
     if (nodes < 1 || nodes > 16 * 64 || numerical_fic) return false;
-    if (model == MODEL_JR) return lanes_rows(nodes) <= 4;  // 8 state variables a node in registers
+    if (model == MODEL_JR) return lanes_rows(nodes, 1024) <= 4;  // 8 state variables a node in registers
     return model == MODEL_RWW || model == MODEL_WC || model == MODEL_RWWEX;
 }
 

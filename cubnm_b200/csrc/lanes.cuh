@@ -63,7 +63,7 @@ __device__ __noinline__ void lanes_states_out(const IntegrateArgs &a, const floa
 // TAN: also the tangent along G (tangent.cuh): ring buffer of (x, dx/dG) pairs,
 // the Balloon-Windkessel tangent beside its state, dBOLD/dG to a.tan_bold.
 template <class M, int NT, int MN, bool DELAY, bool TAN>
-__global__ void __launch_bounds__(NT, 1) k_integrate_lanes(const __grid_constant__ IntegrateArgs a) {
+__global__ void __launch_bounds__(NT, 1024 / NT) k_integrate_lanes(const __grid_constant__ IntegrateArgs a) {
     static_assert(!M::OSC, "phase models run on the per-simulation kernel (numerical FIC too, by the host)");
     using TG = Tangent<M>;
     constexpr int NTG = TAN ? TG::NT : 1;
@@ -250,7 +250,15 @@ cudaError_t launch_model(const IntegrateArgs &a, cudaStream_t st) {
     k_lanes_params<M::NR><<<a.ln_n_groups, 256, 0, st>>>(a, a.ln_params);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    switch (lanes_rows(a.nodes)) {
+    if (a.ln_threads == 512) {  // 32 node rows a CTA, two CTAs an SM: networks of <= 128 nodes
+        switch (lanes_rows(a.nodes, 512)) {
+            case 1: return launch_mn<M, 512, 1, TAN>(a, st);
+            case 2: return launch_mn<M, 512, 2, TAN>(a, st);
+            case 4: return launch_mn<M, 512, 4, TAN>(a, st);
+        }
+        return cudaErrorInvalidValue;
+    }
+    switch (lanes_rows(a.nodes, 1024)) {
         case 1: return launch_mn<M, 1024, 1, TAN>(a, st);
         case 2: return launch_mn<M, 1024, 2, TAN>(a, st);
         case 4: return launch_mn<M, 1024, 4, TAN>(a, st);

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <stdexcept>
@@ -137,6 +138,7 @@ struct Cfg {
     double init_delta = 0.02;
     bool fp32 = false;
     bool philox = false;  // noise segment from Philox on the GPU instead of the host mt19937
+    bool autotune = false;  // pick the FP32 integrator by timing short probe runs (model_config "autotune")
     int nodes = 0, n_sims = 0, time_steps = 0, bold_tr = 0, states_sampling = 0, sim_seed = 0;
     double dt = 0.1, bw_dt = 0.001;
     int bold_len = 0, bold_tr_iters = 0, states_len = 0, states_sampling_iters = 0, bw_it = 0, inner_it = 0;
@@ -178,6 +180,8 @@ static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
             if (v == "fp32") c.fp32 = true;
             else if (v == "fp64") c.fp32 = false;
             else throw Err(CBNM_ERR_CONFIG, "precision must be 'fp64' or 'fp32', got '" + v + "'");
+        } else if (k == "autotune") {
+            c.autotune = to_int(k, v) != 0;
         } else if (k == "noise") {
             if (v == "philox") c.philox = true;
             else if (v == "mt19937") c.philox = false;
@@ -526,9 +530,141 @@ static std::vector<int> pair_tiles(const std::vector<int> &tiles, int n_tiles, i
     return out;
 }
 
+// ---------------------------------------------------------------- FP32 integrator variants
+// The FP32 path has several integrators for the same arithmetic; which is fastest
+// depends on the node count, the delays and the SC's sparsity.  The default
+// choice follows fixed rules (run_impl); with model_config "autotune" = "1" (or
+// CBNM_AUTOTUNE=1) the first run of each workload key times a short probe of
+// every applicable variant on a slice of the batch and keeps the fastest for the
+// process (and in CBNM_TUNE_FILE when set, one "key variant" line each).
+enum Variant { V_DEFAULT = 0, V_PP, V_V5, V_LANES, V_LANES512, V_SIMT, V_COUNT };
+static const char *const kVariantName[V_COUNT] = {"default", "tc2", "tc1", "lanes", "lanes512", "simt"};
+static thread_local int t_force_variant = V_DEFAULT;  // set while a probe runs
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tuned;
+static bool g_tune_loaded = false;
+static Session *g_tune = nullptr;                     // probes run on a session of their own
+static thread_local std::string t_last_variant = "";
+
+static int variant_of(const std::string &name) {
+    for (int v = 0; v < V_COUNT; ++v)
+        if (name == kVariantName[v]) return v;
+    return -1;
+}
+
+static void tune_load() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char *path = std::getenv("CBNM_TUNE_FILE");
+    if (!path) return;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return;
+    char key[512], name[64];
+    while (std::fscanf(f, "%511s %63s", key, name) == 2) {
+        const int v = variant_of(name);
+        if (v > 0) g_tuned[key] = v;
+    }
+    std::fclose(f);
+}
+
+static void tune_store(const std::string &key, int v) {
+    g_tuned[key] = v;
+    const char *path = std::getenv("CBNM_TUNE_FILE");
+    if (!path) return;
+    if (FILE *f = std::fopen(path, "a")) {
+        std::fprintf(f, "%s %s\n", key.c_str(), kVariantName[v]);
+        std::fclose(f);
+    }
+}
+
+static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io, double *tan_bold = nullptr);
+
+// Times one variant on `probe` (host buffers); returns milliseconds of the integrator or -1.
+static double probe_variant(const cbnm_run_args &probe, int v) {
+    const int P = probe.n_sims;
+    cbnm_sizes z;
+    {
+        Cfg c;
+        build_cfg(c, &probe, *find_model(probe.model_name));
+        fill_sizes(c, *find_model(probe.model_name), &z);
+    }
+    std::vector<double> bold((size_t)P * z.bold_len * probe.nodes);
+    std::vector<unsigned char> gb((size_t)std::max(1, z.n_global_out_bool) * P);
+    std::vector<int> gi((size_t)std::max(1, z.n_global_out_int) * P);
+    cbnm_outputs out{};
+    out.sim_bold = bold.data();
+    out.global_bools = gb.data();
+    out.global_ints = gi.data();
+    if (!g_tune) g_tune = new Session();
+    open_session(*g_tune);
+    t_force_variant = v;
+    double best = -1.0;
+    try {
+        for (int rep = 0; rep < 2; ++rep) {  // the first run loads modules and draws the probe's noise
+            run_impl(g_tune, &probe, &out, false);
+            best = g_tune->timing.integrate_ms;
+        }
+    } catch (const Err &) {
+        best = -1.0;  // not applicable to this workload
+    }
+    t_force_variant = V_DEFAULT;
+    return best;
+}
+
+// The tuned variant for this run (probing on first sight of its key).
+static int tuned_variant(const cbnm_run_args *a, const Cfg &c, const std::string &key, const std::vector<int> &cands) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load();
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+    // probe: the first <= 2368 simulations (16 per SM-resident group x 148), <= 1 s, no FC / FCD / states
+    const int P = std::min(c.n_sims, 2368);
+    const int md_g = find_model(a->model_name)->n_global, md_r = find_model(a->model_name)->n_regional;
+    std::vector<double> g((size_t)md_g * P), r((size_t)md_r * P * c.nodes), v(a->v_list, a->v_list + P);
+    for (int q = 0; q < md_g; ++q)
+        std::copy(a->global_params + (size_t)q * c.n_sims, a->global_params + (size_t)q * c.n_sims + P, g.begin() + (size_t)q * P);
+    for (int q = 0; q < md_r; ++q)
+        std::copy(a->regional_params + (size_t)q * c.n_sims * c.nodes,
+                  a->regional_params + (size_t)q * c.n_sims * c.nodes + (size_t)P * c.nodes,
+                  r.begin() + (size_t)q * P * c.nodes);
+    std::vector<std::string> keys, vals;
+    for (int i = 0; i < a->n_config; ++i) {
+        const std::string k = a->config_keys[i];
+        if (k == "do_fc" || k == "do_fcd" || k == "autotune") continue;
+        keys.push_back(k);
+        vals.push_back(a->config_values[i]);
+    }
+    keys.push_back("do_fc"); vals.push_back("0");
+    keys.push_back("do_fcd"); vals.push_back("0");
+    std::vector<const char *> kp, vp;
+    for (size_t i = 0; i < keys.size(); ++i) { kp.push_back(keys[i].c_str()); vp.push_back(vals[i].c_str()); }
+    cbnm_run_args probe = *a;
+    probe.n_sims = P;
+    probe.global_params = g.data();
+    probe.regional_params = r.data();
+    probe.v_list = v.data();
+    probe.config_keys = kp.data();
+    probe.config_values = vp.data();
+    probe.n_config = (int)kp.size();
+    probe.ext_out = 0;
+    probe.states_ts = 0;
+    probe.noise_out = 0;
+    probe.force_reinit = 0;
+    const int tr = std::max(1, a->bold_tr);
+    probe.time_steps = std::min(a->time_steps, std::max(tr, (1000 / tr) * tr));
+    int best_v = V_DEFAULT;
+    double best_ms = 0.0;
+    for (int cand : cands) {
+        const double ms = probe_variant(probe, cand);
+        if (ms > 0.0 && (best_v == V_DEFAULT || ms < best_ms)) { best_v = cand; best_ms = ms; }
+    }
+    if (best_v != V_DEFAULT) tune_store(key, best_v);
+    return best_v;
+}
+
 // tan_bold (device, [N][bold_len][nodes]) non-null: also integrate the tangent along
 // G and write dBOLD/dG there (lane kernel, FP32 precision, rWW or WC).
-static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io, double *tan_bold = nullptr) {
+static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool device_io, double *tan_bold) {
     const double t_begin = now_s();
     check_args(a);
     if (!o || !o->sim_bold) throw Err(CBNM_ERR_ARG, "null output arrays");
@@ -658,10 +794,36 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     if (tan_bold && (!c.fp32 || !lanes_tangent_supported(md.id) || num_fic || !lanes_supported(md.id, n, num_fic)))
         throw Err(CBNM_ERR_UNSUPPORTED, "the G tangent needs precision fp32, model rWW or WC, at most 1024 nodes and "
                                         "no numerical FIC");
-    const bool use_tc = !tan_bold && c.fp32 && !force_simt && fp32_supported(md.id, n, has_delay) && !num_fic;
-    bool use_lanes = c.fp32 && (!force_simt || tan_bold) && !use_tc && lanes_supported(md.id, n, num_fic) &&
-                     (has_delay ? *std::max_element(h_max_delay.begin(), h_max_delay.end()) + 1 : 2) * (long long)n <
-                         (1LL << 30);
+    const bool tc_ok = c.fp32 && fp32_supported(md.id, n, has_delay) && !num_fic;
+    const bool lanes_ok = c.fp32 && lanes_supported(md.id, n, num_fic) &&
+                          (has_delay ? *std::max_element(h_max_delay.begin(), h_max_delay.end()) + 1 : 2) * (long long)n <
+                              (1LL << 30);
+    int variant = t_force_variant;
+    if (variant == V_DEFAULT && !tan_bold && c.fp32 && !force_simt && !device_io &&
+        (c.autotune || (std::getenv("CBNM_AUTOTUNE") && std::string(std::getenv("CBNM_AUTOTUNE")) == "1"))) {
+        std::vector<int> cands;
+        if (tc_ok && pp_supported(md.id, n, has_delay)) cands.push_back(V_PP);
+        if (tc_ok) cands.push_back(V_V5);
+        if (lanes_ok) cands.push_back(V_LANES);
+        if (lanes_ok && n <= 128) cands.push_back(V_LANES512);
+        cands.push_back(V_SIMT);
+        const int Dmax = has_delay ? *std::max_element(h_max_delay.begin(), h_max_delay.end()) : 0;
+        const std::string key = std::string(md.name) + "|n" + std::to_string(n) + "|D" + std::to_string(Dmax) +
+                                "|scs" + std::to_string(a->n_scs) + "|nfic" + std::to_string((int)num_fic);
+        variant = tuned_variant(a, c, key, cands);
+    }
+    if (variant != V_DEFAULT) {  // a forced or tuned variant must apply to this run
+        const bool ok = c.fp32 && !tan_bold &&
+                        ((variant == V_PP && tc_ok && pp_supported(md.id, n, has_delay)) || (variant == V_V5 && tc_ok) ||
+                         (variant == V_LANES && lanes_ok) || (variant == V_LANES512 && lanes_ok && n <= 128) ||
+                         variant == V_SIMT);
+        if (!ok) throw Err(CBNM_ERR_UNSUPPORTED, std::string("integrator variant ") + kVariantName[variant] +
+                                                     " does not apply to this run");
+    }
+    const bool use_tc = variant == V_DEFAULT ? (!tan_bold && !force_simt && tc_ok) : (variant == V_PP || variant == V_V5);
+    bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (!force_simt || tan_bold) && !use_tc)
+                                          : (variant == V_LANES || variant == V_LANES512);
+    const int lanes_threads = variant == V_LANES512 ? 512 : 1024;
     if (has_delay) {
         S.d_delay.ensure(sizeof(int) * h_delay.size());
         CK(cudaMemcpyAsync(S.d_delay.p, h_delay.data(), sizeof(int) * h_delay.size(), cudaMemcpyHostToDevice, S.st));
@@ -838,7 +1000,8 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     // rWW on the tensor cores: the two-tile kernel unless CBNM_FP32_TC=v5 selects the
     // single-tile one
     const char *tc_kind = std::getenv("CBNM_FP32_TC");
-    const bool use_pp = use_tc && pp_supported(md.id, n, has_delay) && !(tc_kind && std::string(tc_kind) == "v5");
+    const bool use_pp = use_tc && pp_supported(md.id, n, has_delay) &&
+                        (variant == V_DEFAULT ? !(tc_kind && std::string(tc_kind) == "v5") : variant == V_PP);
     if (use_tc) {
         // tiles of simulations that share one SC
         const int TN = use_pp ? 32 : fp32_tile_for(n);
@@ -911,7 +1074,8 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
             for (; cnt < G; ++cnt) groups.push_back(-1);
         }
         ia.ln_n_groups = (int)(groups.size() / (3 + G));
-        ia.ln_grid = std::min(ia.ln_n_groups, sm_count());
+        ia.ln_threads = lanes_threads;
+        ia.ln_grid = std::min(ia.ln_n_groups, sm_count() * (1024 / lanes_threads));
         S.d_ln_groups.ensure(sizeof(int) * groups.size());
         CK(cudaMemcpyAsync(S.d_ln_groups.p, groups.data(), sizeof(int) * groups.size(), cudaMemcpyHostToDevice, S.st));
         ia.ln_groups = S.d_ln_groups.as<int>();
@@ -933,6 +1097,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         CK(launch_integrate_fp64(md.id, ia, S.st));
         ++launches;
     }
+    t_last_variant = !c.fp32 ? "fp64" : use_pp ? "tc2" : use_tc ? "tc1" : use_lanes ? (lanes_threads == 512 ? "lanes512" : "lanes") : "simt";
     CK(cudaEventRecord(S.ev[2], S.st));
     if (!device_io) {  // the integrator runs asynchronously: map the host output pages meanwhile
         prefault_host(o->sim_bold, sizeof(double) * bold_n);
@@ -1368,6 +1533,15 @@ int cbnm_reset(void) {
 }
 
 const char *cbnm_last_error(void) { return g_err.c_str(); }
+
+const char *cbnm_last_integrator(void) { return t_last_variant.c_str(); }
+
+int cbnm_tune_reset(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned.clear();
+    g_tune_loaded = false;
+    return CBNM_OK;
+}
 
 int cbnm_gof(const double *sim_fc, int n_sims, int n_pairs, const double *emp_fc, const double *sim_fcd,
              int n_window_pairs, const double *emp_fcd, int n_emp_fcd, double *fc_corr, double *fc_diff,

@@ -186,6 +186,21 @@ int cbnm_reset(void);
 /* Human-readable description of the last error (empty if none). */
 const char *cbnm_last_error(void);
 
+/* Integrator of the last run on this thread: "fp64", or for precision "fp32"
+ * "tc2" (two-tile tensor-core kernel), "tc1" (single-tile tensor-core kernel),
+ * "lanes" / "lanes512" (simulations on the lanes, 1024 / 512 threads a CTA) or
+ * "simt" (one CTA per simulation).  No reference counterpart (diagnostic). */
+const char *cbnm_last_integrator(void);
+
+/* Forgets the autotuner's choices (model_config "autotune" = "1" or
+ * CBNM_AUTOTUNE=1: the first run of each workload -- model, nodes, largest
+ * delay, number of SCs -- times a short probe of every applicable FP32
+ * integrator on up to 2,368 of its simulations and keeps the fastest; with
+ * CBNM_TUNE_FILE set the choices are also appended to and read from that file).
+ * Forced variants for testing: CBNM_FP32_KERNEL / CBNM_FP32_TC.  No reference
+ * counterpart: the reference has one kernel. */
+int cbnm_tune_reset(void);
+
 /* Goodness-of-fit seam (src/cubnm/utils.py:416-507 fc_corr_device and
  * :306-414 fcd_ks_device; src/cubnm/sim/base.py:1165-1189 for fc_diff and
  * fc_normec).  Host arrays; all outputs [n_sims].
