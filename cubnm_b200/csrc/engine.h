@@ -141,6 +141,13 @@ bool lanes_supported(int model, int nodes, bool numerical_fic);
 bool lanes_tangent_supported(int model);
 int lanes_rows(int nodes, int threads);
 cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st);
+// The parameter layout of a run (first half of launch_integrate_lanes), and one
+// persistent launch over the 16-simulation groups of several runs of one model:
+// items [n_items] = (run, group), longest first; scratch per CTA for the largest run.
+cudaError_t launch_integrate_lanes_params(int model, const IntegrateArgs &a, cudaStream_t st);
+cudaError_t launch_integrate_lanes_multi(int model, const IntegrateArgs *runs, const int2 *items, int n_items,
+                                         int *counter, int mn, int grid, float *hist, long long hist_per_cta,
+                                         double *bw, long long bw_per_cta, cudaStream_t st);
 bool fp32_supported(int model, int nodes, bool has_delay);
 // Two-tile tensor-core kernel (integrate_pp.cu): rWW, no delays, <= 128 nodes.
 // Work items: [n_tiles][1 + 64] = SC index, then 32 simulation ids per half (-1 = empty).

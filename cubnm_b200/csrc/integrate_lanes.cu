@@ -20,6 +20,36 @@ bool lanes_supported(int model, int nodes, bool numerical_fic) {
 
 cudaError_t launch_integrate_lanes_tan(int model, const IntegrateArgs &a, cudaStream_t st);  // integrate_lanes_tan.cu
 
+cudaError_t launch_integrate_lanes_params(int model, const IntegrateArgs &a, cudaStream_t st) {
+    switch (model) {
+        case MODEL_RWW: return lanes::launch_params<RWWm<float>>(a, st);
+        case MODEL_WC: return lanes::launch_params<WCm<float>>(a, st);
+        case MODEL_JR: return lanes::launch_params<JRm<float>>(a, st);
+        case MODEL_RWWEX: return lanes::launch_params<RWWExm<float>>(a, st);
+    }
+    return cudaErrorNotSupported;
+}
+
+cudaError_t launch_integrate_lanes_multi(int model, const IntegrateArgs *runs, const int2 *items, int n_items,
+                                         int *counter, int mn, int grid, float *hist, long long hist_per_cta,
+                                         double *bw, long long bw_per_cta, cudaStream_t st) {
+    switch (model) {
+        case MODEL_RWW:
+            return lanes::launch_multi<RWWm<float>>(runs, items, n_items, counter, mn, grid, hist, hist_per_cta, bw,
+                                                    bw_per_cta, st);
+        case MODEL_WC:
+            return lanes::launch_multi<WCm<float>>(runs, items, n_items, counter, mn, grid, hist, hist_per_cta, bw,
+                                                   bw_per_cta, st);
+        case MODEL_JR:
+            return lanes::launch_multi<JRm<float>>(runs, items, n_items, counter, mn, grid, hist, hist_per_cta, bw,
+                                                   bw_per_cta, st);
+        case MODEL_RWWEX:
+            return lanes::launch_multi<RWWExm<float>>(runs, items, n_items, counter, mn, grid, hist, hist_per_cta, bw,
+                                                      bw_per_cta, st);
+    }
+    return cudaErrorNotSupported;
+}
+
 cudaError_t launch_integrate_lanes(int model, const IntegrateArgs &a, cudaStream_t st) {
     if (a.tan_bold) return launch_integrate_lanes_tan(model, a, st);
     switch (model) {

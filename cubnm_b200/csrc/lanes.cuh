@@ -62,8 +62,9 @@ __device__ __noinline__ void lanes_states_out(const IntegrateArgs &a, const floa
 
 // TAN: also the tangent along G (tangent.cuh): ring buffer of (x, dx/dG) pairs,
 // the Balloon-Windkessel tangent beside its state, dBOLD/dG to a.tan_bold.
-template <class M, int NT, int MN, bool DELAY, bool TAN>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_integrate_lanes(const __grid_constant__ IntegrateArgs a) {
+template <class M, int NT, int MN, int DMODE, bool TAN>
+__device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
+                                            typename std::conditional<TAN, float2, float>::type *hist, double *bws) {
     static_assert(!M::OSC, "phase models run on the per-simulation kernel (numerical FIC too, by the host)");
     using TG = Tangent<M>;
     constexpr int NTG = TAN ? TG::NT : 1;
@@ -79,144 +80,179 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_integrate_lanes(const __grid_
     const size_t rstride = (size_t)a.n_sims * n;
     const size_t ext = a.states_ts ? (size_t)n * a.states_len : (size_t)n;
     const BW64 &bw = a.bwf;
-    H *hist = reinterpret_cast<H *>(a.ln_hist + (size_t)blockIdx.x * a.ln_hist_per_cta);
-    double *bws = a.ln_bw + (size_t)blockIdx.x * n * BWW * LN_SIMS;
+    // DMODE 0: no delays, 1: delays, 2: as the run says (a.has_delay); without delays
+    // the coupling reads the previous step, one slot back
+    const bool delayed = DMODE == 1 || (DMODE == 2 && a.has_delay);
+    const int *gd = a.ln_groups + (size_t)gi * (3 + LN_SIMS);
+    const int sc_i = gd[0], table = gd[1], D = gd[2];   // D: the group's largest delay (1 without delays)
+    const int sim = gd[3 + s];
+    const bool live = sim >= 0;
+    const float *par = a.ln_params + (size_t)gi * n * M::NR * LN_SIMS;
+    const int2 *ell = a.ell_pk32 + (size_t)(sc_i * a.ell_tables + table) * EK * n;
+    R g[M::NG], iv[M::NI], st[MN][M::NS], dst[MN][NTG];
+#pragma unroll
+    for (int i = 0; i < M::NG; ++i) g[i] = live ? (R)a.gparams[(size_t)i * a.n_sims + sim] : R(0);
+#pragma unroll
+    for (int i = 0; i < M::NI; ++i) iv[i] = R(0);
+    const int slots = D + 1, hw = slots * n;
+#pragma unroll
+    for (int m = 0; m < MN; ++m) {
+        const int j = r0 + ROW * m;
+#pragma unroll
+        for (int v = 0; v < M::NS; ++v) st[m][v] = R(0);
+#pragma unroll
+        for (int v = 0; v < NTG; ++v) dst[m][v] = R(0);
+        if (j >= n) continue;
+        R r[M::NR];
+#pragma unroll
+        for (int q = 0; q < M::NR; ++q) r[q] = par[((size_t)j * M::NR + q) * LN_SIMS + s];
+        M::init(st[m], iv, g, r);
+        for (int b = 0; b < slots; ++b) hist[((size_t)b * n + j) * LN_SIMS + s] = hval<TAN>(st[m][M::CONN], 0.0f);
+        double *bj = bws + (size_t)j * BWW * LN_SIMS + s;
+        bj[0] = 0.0;
+        bj[LN_SIMS] = 1.0;
+        bj[2 * LN_SIMS] = 1.0;
+        bj[3 * LN_SIMS] = 1.0;
+        if (TAN)
+            for (int c = 4; c < 8; ++c) bj[c * LN_SIMS] = 0.0;
+        if (live && a.ext_out && !a.states_ts)
+            for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] = 0.0;
+    }
+    __syncthreads();
 
-    for (int gi = blockIdx.x; gi < a.ln_n_groups; gi += gridDim.x) {
-        const int *gd = a.ln_groups + (size_t)gi * (3 + LN_SIMS);
-        const int sc_i = gd[0], table = gd[1], D = gd[2];   // D: the group's largest delay (1 without delays)
-        const int sim = gd[3 + s];
-        const bool live = sim >= 0;
-        const float *par = a.ln_params + (size_t)gi * n * M::NR * LN_SIMS;
-        const int2 *ell = a.ell_pk32 + (size_t)(sc_i * a.ell_tables + table) * EK * n;
-        R g[M::NG], iv[M::NI], st[MN][M::NS], dst[MN][NTG];
+    int buff = D, bold_i = 0, states_i = 0, repeat = 0;
+    int shj[MN];
 #pragma unroll
-        for (int i = 0; i < M::NG; ++i) g[i] = live ? (R)a.gparams[(size_t)i * a.n_sims + sim] : R(0);
-#pragma unroll
-        for (int i = 0; i < M::NI; ++i) iv[i] = R(0);
-        const int slots = D + 1, hw = slots * n;
-#pragma unroll
-        for (int m = 0; m < MN; ++m) {
-            const int j = r0 + ROW * m;
-#pragma unroll
-            for (int v = 0; v < M::NS; ++v) st[m][v] = R(0);
-#pragma unroll
-            for (int v = 0; v < NTG; ++v) dst[m][v] = R(0);
-            if (j >= n) continue;
-            R r[M::NR];
-#pragma unroll
-            for (int q = 0; q < M::NR; ++q) r[q] = par[((size_t)j * M::NR + q) * LN_SIMS + s];
-            M::init(st[m], iv, g, r);
-            for (int b = 0; b < slots; ++b) hist[((size_t)b * n + j) * LN_SIMS + s] = hval<TAN>(st[m][M::CONN], 0.0f);
-            double *bj = bws + (size_t)j * BWW * LN_SIMS + s;
-            bj[0] = 0.0;
-            bj[LN_SIMS] = 1.0;
-            bj[2 * LN_SIMS] = 1.0;
-            bj[3 * LN_SIMS] = 1.0;
-            if (TAN)
-                for (int c = 4; c < 8; ++c) bj[c * LN_SIMS] = 0.0;
-            if (live && a.ext_out && !a.states_ts)
-                for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] = 0.0;
-        }
-        __syncthreads();
-
-        int buff = D, bold_i = 0, states_i = 0, repeat = 0;
-        int shj[MN];
-#pragma unroll
-        for (int m = 0; m < MN; ++m) shj[m] = (r0 + ROW * m < n) ? a.sh_nodes[r0 + ROW * m] : 0;
-        double *bold = a.bold + (size_t)(live ? sim : 0) * a.bold_len * n;
-        for (int bw_i = 0; bw_i < a.bw_it; ++bw_i) {
-            const int sh_ts = a.sh_ts[(bw_i % a.noise_bw_it) + repeat * a.noise_bw_it];
-            const bool sample = a.ext_out && (bw_i + 1) % a.states_sampling_iters == 0;  // bnm.cpp:337-355
-            for (int inner = 0; inner < a.inner_it; ++inner) {
-                const int hbase = buff * n;
-                const bool out_now = sample && live && inner == a.inner_it - 1;
-#pragma unroll
-                for (int m = 0; m < MN; ++m) {
-                    const int j = r0 + ROW * m;
-                    if (j >= n) continue;
-                    // coupling: sum over the nonzeros of column j of SC[k][j] x_k(t - d_kj)
-                    const int2 *pk = ell + j;
-                    R in = R(0), din = R(0);
-#pragma unroll 4
-                    for (int q = 0; q < EK; ++q) {
-                        const int2 e = __ldg(pk + (size_t)q * n);
-                        int h = hbase + e.x + (DELAY ? 0 : n);
-                        if (h >= hw) h -= hw;
-                        const H xk = hist[(size_t)h * LN_SIMS + s];
-                        if constexpr (TAN) {
-                            in += __int_as_float(e.y) * xk.x;
-                            din += __int_as_float(e.y) * xk.y;
-                        } else {
-                            in += __int_as_float(e.y) * xk;
-                        }
-                    }
-                    const long long ni = ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
-                    const R n0 = __ldg(a.noise_f32 + ni);
-                    const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
-                    R r[M::NR];
-#pragma unroll
-                    for (int q = 0; q < M::NR; ++q) r[q] = __ldg(par + ((size_t)j * M::NR + q) * LN_SIMS + s);
-                    if constexpr (TAN) TG::step(st[m], dst[m], iv, g, r, in, din, n0, n1, a.K);
-                    else M::step(st[m], iv, g, r, in, n0, n1, a.K);
-                    if (out_now) lanes_states_out<M::NS>(a, st[m], sim, j, states_i);
-                }
-#pragma unroll
-                for (int m = 0; m < MN; ++m) {
-                    const int j = r0 + ROW * m;
-                    if (j < n) hist[((size_t)hbase + j) * LN_SIMS + s] = hval<TAN>(st[m][M::CONN], dst[m][TAN ? TG::CONN_T : 0]);
-                }
-                __syncthreads();  // this step's slot is written before the next step reads it
-                buff = buff ? buff - 1 : D;
-            }
-            // Balloon-Windkessel (bw.cu:4-15), BOLD at TR (bnm.cpp:316-335)
-            const bool tr = (bw_i + 1) % a.bold_tr_iters == 0;
-#pragma unroll
-            for (int m = 0; m < MN; ++m) {
-                const int j = r0 + ROW * m;
-                if (j >= n || !live) continue;
-                double *bj = bws + (size_t)j * BWW * LN_SIMS + s;
-                double x = bj[0], f = bj[LN_SIMS], nu = bj[2 * LN_SIMS], q = bj[3 * LN_SIMS];
-                if constexpr (TAN) {
-                    double dx = bj[4 * LN_SIMS], df = bj[5 * LN_SIMS], dnu = bj[6 * LN_SIMS], dq = bj[7 * LN_SIMS];
-                    bw_tangent64(x, f, nu, q, dx, df, dnu, dq, (double)dst[m][TG::CONN_T], bw);
-                    bj[4 * LN_SIMS] = dx;
-                    bj[5 * LN_SIMS] = df;
-                    bj[6 * LN_SIMS] = dnu;
-                    bj[7 * LN_SIMS] = dq;
-                    bw_step64(x, f, nu, q, (double)st[m][M::BOLDV], bw);
-                    if (tr && bold_i < a.bold_len)  // dBOLD = V0 (-k1 dq - k2 (dq / nu - q dnu / nu^2) - k3 dnu)
-                        a.tan_bold[(size_t)sim * a.bold_len * n + (size_t)bold_i * n + j] =
-                            -bw.V0k1 * dq - bw.V0k2 * (dq / nu - q * dnu / (nu * nu)) - bw.V0k3 * dnu;
-                } else {
-                    bw_step64(x, f, nu, q, (double)st[m][M::BOLDV], bw);
-                }
-                bj[0] = x;
-                bj[LN_SIMS] = f;
-                bj[2 * LN_SIMS] = nu;
-                bj[3 * LN_SIMS] = q;
-                if (tr && bold_i < a.bold_len)  // no slot for a sample past bold_len
-                    bold[(size_t)bold_i * n + j] = bw.V0k1 * (1 - q) + bw.V0k2 * (1 - q / nu) + bw.V0k3 * (1 - nu);
-            }
-            if (tr) bold_i++;
-            if (sample) states_i++;
-            if ((bw_i + 1) % a.noise_bw_it == 0 && bw_i + 1 < a.bw_it) {
-                repeat++;
-#pragma unroll
-                for (int m = 0; m < MN; ++m)
-                    if (r0 + ROW * m < n) shj[m] = a.sh_nodes[(size_t)repeat * n + r0 + ROW * m];
-            }
-        }
-        if (live && a.ext_out && !a.states_ts) {
-            const int pts = states_i - a.n_states_samples_remove;
+    for (int m = 0; m < MN; ++m) shj[m] = (r0 + ROW * m < n) ? a.sh_nodes[r0 + ROW * m] : 0;
+    double *bold = a.bold + (size_t)(live ? sim : 0) * a.bold_len * n;
+    for (int bw_i = 0; bw_i < a.bw_it; ++bw_i) {
+        const int sh_ts = a.sh_ts[(bw_i % a.noise_bw_it) + repeat * a.noise_bw_it];
+        const bool sample = a.ext_out && (bw_i + 1) % a.states_sampling_iters == 0;  // bnm.cpp:337-355
+        for (int inner = 0; inner < a.inner_it; ++inner) {
+            const int hbase = buff * n;
+            const bool out_now = sample && live && inner == a.inner_it - 1;
 #pragma unroll
             for (int m = 0; m < MN; ++m) {
                 const int j = r0 + ROW * m;
                 if (j >= n) continue;
-                for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] /= pts;
+                // coupling: sum over the nonzeros of column j of SC[k][j] x_k(t - d_kj)
+                const int2 *pk = ell + j;
+                R in = R(0), din = R(0);
+#pragma unroll 4
+                for (int q = 0; q < EK; ++q) {
+                    const int2 e = __ldg(pk + (size_t)q * n);
+                    int h = hbase + e.x + (delayed ? 0 : n);
+                    if (h >= hw) h -= hw;
+                    const H xk = hist[(size_t)h * LN_SIMS + s];
+                    if constexpr (TAN) {
+                        in += __int_as_float(e.y) * xk.x;
+                        din += __int_as_float(e.y) * xk.y;
+                    } else {
+                        in += __int_as_float(e.y) * xk;
+                    }
+                }
+                const long long ni = ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
+                const R n0 = __ldg(a.noise_f32 + ni);
+                const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
+                R r[M::NR];
+#pragma unroll
+                for (int q = 0; q < M::NR; ++q) r[q] = __ldg(par + ((size_t)j * M::NR + q) * LN_SIMS + s);
+                if constexpr (TAN) TG::step(st[m], dst[m], iv, g, r, in, din, n0, n1, a.K);
+                else M::step(st[m], iv, g, r, in, n0, n1, a.K);
+                if (out_now) lanes_states_out<M::NS>(a, st[m], sim, j, states_i);
             }
+#pragma unroll
+            for (int m = 0; m < MN; ++m) {
+                const int j = r0 + ROW * m;
+                if (j < n) hist[((size_t)hbase + j) * LN_SIMS + s] = hval<TAN>(st[m][M::CONN], dst[m][TAN ? TG::CONN_T : 0]);
+            }
+            __syncthreads();  // this step's slot is written before the next step reads it
+            buff = buff ? buff - 1 : D;
         }
-        __syncthreads();  // the next group reuses the ring buffer and the Balloon-Windkessel scratch
+        // Balloon-Windkessel (bw.cu:4-15), BOLD at TR (bnm.cpp:316-335)
+        const bool tr = (bw_i + 1) % a.bold_tr_iters == 0;
+#pragma unroll
+        for (int m = 0; m < MN; ++m) {
+            const int j = r0 + ROW * m;
+            if (j >= n || !live) continue;
+            double *bj = bws + (size_t)j * BWW * LN_SIMS + s;
+            double x = bj[0], f = bj[LN_SIMS], nu = bj[2 * LN_SIMS], q = bj[3 * LN_SIMS];
+            if constexpr (TAN) {
+                double dx = bj[4 * LN_SIMS], df = bj[5 * LN_SIMS], dnu = bj[6 * LN_SIMS], dq = bj[7 * LN_SIMS];
+                bw_tangent64(x, f, nu, q, dx, df, dnu, dq, (double)dst[m][TG::CONN_T], bw);
+                bj[4 * LN_SIMS] = dx;
+                bj[5 * LN_SIMS] = df;
+                bj[6 * LN_SIMS] = dnu;
+                bj[7 * LN_SIMS] = dq;
+                bw_step64(x, f, nu, q, (double)st[m][M::BOLDV], bw);
+                if (tr && bold_i < a.bold_len)  // dBOLD = V0 (-k1 dq - k2 (dq / nu - q dnu / nu^2) - k3 dnu)
+                    a.tan_bold[(size_t)sim * a.bold_len * n + (size_t)bold_i * n + j] =
+                        -bw.V0k1 * dq - bw.V0k2 * (dq / nu - q * dnu / (nu * nu)) - bw.V0k3 * dnu;
+            } else {
+                bw_step64(x, f, nu, q, (double)st[m][M::BOLDV], bw);
+            }
+            bj[0] = x;
+            bj[LN_SIMS] = f;
+            bj[2 * LN_SIMS] = nu;
+            bj[3 * LN_SIMS] = q;
+            if (tr && bold_i < a.bold_len)  // no slot for a sample past bold_len
+                bold[(size_t)bold_i * n + j] = bw.V0k1 * (1 - q) + bw.V0k2 * (1 - q / nu) + bw.V0k3 * (1 - nu);
+        }
+        if (tr) bold_i++;
+        if (sample) states_i++;
+        if ((bw_i + 1) % a.noise_bw_it == 0 && bw_i + 1 < a.bw_it) {
+            repeat++;
+#pragma unroll
+            for (int m = 0; m < MN; ++m)
+                if (r0 + ROW * m < n) shj[m] = a.sh_nodes[(size_t)repeat * n + r0 + ROW * m];
+        }
+    }
+    if (live && a.ext_out && !a.states_ts) {
+        const int pts = states_i - a.n_states_samples_remove;
+#pragma unroll
+        for (int m = 0; m < MN; ++m) {
+            const int j = r0 + ROW * m;
+            if (j >= n) continue;
+            for (int v = 0; v < M::NS; ++v) a.states[((size_t)v * a.n_sims + sim) * ext + j] /= pts;
+        }
+    }
+    __syncthreads();  // the next group reuses the ring buffer and the Balloon-Windkessel scratch
+}
+
+// One run: CTA b integrates groups b, b + grid, ... of the run.
+template <class M, int NT, int MN, bool DELAY, bool TAN>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_integrate_lanes(const __grid_constant__ IntegrateArgs a) {
+    using H = typename std::conditional<TAN, float2, float>::type;
+    H *hist = reinterpret_cast<H *>(a.ln_hist + (size_t)blockIdx.x * a.ln_hist_per_cta);
+    double *bws = a.ln_bw + (size_t)blockIdx.x * a.nodes * (TAN ? 8 : 4) * LN_SIMS;
+    for (int gi = blockIdx.x; gi < a.ln_n_groups; gi += gridDim.x)
+        lanes_group<M, NT, MN, DELAY ? 1 : 0, TAN>(a, gi, hist, bws);
+}
+
+// Several runs in one launch (the groups of an uneven batch): a work queue of
+// (run, group) items, longest first, taken by persistent CTAs from an atomic
+// counter; the run's arguments are copied into shared memory per item.  The
+// ring-buffer and Balloon-Windkessel scratch are per CTA, sized for the largest run.
+template <class M, int NT, int MN>
+__global__ void __launch_bounds__(NT, 1024 / NT)
+    k_integrate_lanes_multi(const IntegrateArgs *runs, const int2 *items, int n_items, int *counter, float *hist,
+                            long long hist_per_cta, double *bw, long long bw_per_cta) {
+    __shared__ IntegrateArgs sa;
+    __shared__ int s_item;
+    float *h = hist + (size_t)blockIdx.x * hist_per_cta;
+    double *b = bw + (size_t)blockIdx.x * bw_per_cta;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const int2 w = items[it];
+        const int *src = reinterpret_cast<const int *>(runs + w.x);
+        int *dst = reinterpret_cast<int *>(&sa);
+        for (int k = threadIdx.x; k < (int)(sizeof(IntegrateArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+        lanes_group<M, NT, MN, 2, false>(sa, w.y, h, b);
+        __syncthreads();  // the next item reuses the scratch and the shared arguments
     }
 }
 
@@ -245,6 +281,12 @@ cudaError_t launch_mn(const IntegrateArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class M>
+cudaError_t launch_params(const IntegrateArgs &a, cudaStream_t st) {
+    k_lanes_params<M::NR><<<a.ln_n_groups, 256, 0, st>>>(a, a.ln_params);
+    return cudaGetLastError();
+}
+
 template <class M, bool TAN>
 cudaError_t launch_model(const IntegrateArgs &a, cudaStream_t st) {
     k_lanes_params<M::NR><<<a.ln_n_groups, 256, 0, st>>>(a, a.ln_params);
@@ -270,6 +312,27 @@ cudaError_t launch_model(const IntegrateArgs &a, cudaStream_t st) {
             break;
     }
     return cudaErrorInvalidValue;
+}
+
+template <class M>
+cudaError_t launch_multi(const IntegrateArgs *runs, const int2 *items, int n_items, int *counter, int mn, int grid,
+                         float *hist, long long hist_per_cta, double *bw, long long bw_per_cta, cudaStream_t st) {
+#define CBNM_LANES_MULTI(MNV) \
+    k_integrate_lanes_multi<M, 1024, MNV><<<grid, 1024, 0, st>>>(runs, items, n_items, counter, hist, hist_per_cta, bw, bw_per_cta)
+    switch (mn) {
+        case 1: CBNM_LANES_MULTI(1); break;
+        case 2: CBNM_LANES_MULTI(2); break;
+        case 4: CBNM_LANES_MULTI(4); break;
+        case 8:
+            if constexpr (M::NS <= 6) { CBNM_LANES_MULTI(8); break; }
+            return cudaErrorInvalidValue;
+        case 16:
+            if constexpr (M::NS <= 6) { CBNM_LANES_MULTI(16); break; }
+            return cudaErrorInvalidValue;
+        default: return cudaErrorInvalidValue;
+    }
+#undef CBNM_LANES_MULTI
+    return cudaGetLastError();
 }
 
 }  // namespace lanes

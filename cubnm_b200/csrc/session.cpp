@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <condition_variable>
 #include <mutex>
 #include <numeric>
 #include <random>
@@ -386,7 +387,10 @@ static void close_session(Session *&p) {
     p = nullptr;
 }
 
+static void release_batch_launch();  // below, with the batch machinery
+
 static void release_session() {
+    release_batch_launch();
     close_session(g_sess);
     for (Session *&b : g_batch) close_session(b);
     g_batch.clear();
@@ -528,6 +532,126 @@ static std::vector<int> pair_tiles(const std::vector<int> &tiles, int n_tiles, i
     *n_items = count();
     *grid = std::max(1, std::min(sms, count()));
     return out;
+}
+
+// ---------------------------------------------------------------- one launch for a batch's lane groups
+// cbnm_run_batch runs up to 16 groups at a time ("a round"), each in a worker
+// thread with its own session.  Groups that take the lane kernel (FP32, delays or
+// > 128 nodes) do not launch it themselves: each prepares its inputs, lays out
+// its parameters on its own stream and joins the round; when every group of the
+// round has joined or declined (taken another integrator, or failed), the last
+// one launches a single persistent work-queue kernel over all joined groups'
+// 16-simulation items, longest first, and the joined groups then continue with
+// their FC / FCD and copies once that kernel is done.
+struct BatchRound {
+    std::mutex mu;
+    std::condition_variable cv;
+    int expected = 0, resolved = 0;
+    bool launched = false;
+    std::string err;
+    struct Join {
+        IntegrateArgs ia;
+        int model;
+        cudaEvent_t ready;
+    };
+    std::vector<Join> joins;
+};
+struct BatchLaunch {  // state shared by the rounds of one cbnm_run_batch call (they run in order)
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+    DBuf runs, items, counter, hist, bw;
+    std::vector<std::vector<IntegrateArgs>> host_runs;   // kept alive for the asynchronous copies
+    std::vector<std::vector<int2>> host_items;
+    float kernel_ms = 0.0f;
+    int launches = 0;
+};
+static thread_local BatchRound *t_round = nullptr;
+static thread_local bool t_round_resolved = false;
+static BatchLaunch *g_batch_launch = nullptr;
+
+// Launches the round's combined kernel(s), one per model (called with the round's lock held).
+static void round_launch(BatchRound &R) {
+    BatchLaunch &B = *g_batch_launch;
+    try {
+        std::map<int, std::vector<int>> by_model;
+        for (int i = 0; i < (int)R.joins.size(); ++i) by_model[R.joins[i].model].push_back(i);
+        for (const auto &kv : by_model) {
+            std::vector<IntegrateArgs> runs;
+            std::vector<std::pair<double, int2>> work;
+            long long hist_per = 0, bw_per = 0;
+            int mn = 1;
+            for (int i : kv.second) {
+                const IntegrateArgs &ia = R.joins[i].ia;
+                CK(cudaStreamWaitEvent(B.st, R.joins[i].ready, 0));
+                const int r = (int)runs.size();
+                runs.push_back(ia);
+                const double cost = (double)ia.nodes * std::max(1, ia.ell_k) * ia.bw_it * ia.inner_it;
+                for (int gi = 0; gi < ia.ln_n_groups; ++gi) work.push_back({cost, make_int2(r, gi)});
+                hist_per = std::max(hist_per, ia.ln_hist_per_cta);
+                bw_per = std::max(bw_per, (long long)ia.nodes * 4 * 16);
+                mn = std::max(mn, lanes_rows(ia.nodes, 1024));
+            }
+            std::stable_sort(work.begin(), work.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+            std::vector<int2> items;
+            for (const auto &w : work) items.push_back(w.second);
+            const int grid = std::min((int)items.size(), sm_count());
+            B.host_runs.push_back(std::move(runs));
+            B.host_items.push_back(std::move(items));
+            const auto &hr = B.host_runs.back();
+            const auto &hi = B.host_items.back();
+            CK(cudaStreamSynchronize(B.st));  // the scratch of the previous launch is free
+            IntegrateArgs *d_runs = (IntegrateArgs *)B.runs.ensure(sizeof(IntegrateArgs) * hr.size());
+            int2 *d_items = (int2 *)B.items.ensure(sizeof(int2) * hi.size());
+            int *d_counter = (int *)B.counter.ensure(sizeof(int));
+            float *d_hist = (float *)B.hist.ensure(sizeof(float) * (size_t)grid * hist_per);
+            double *d_bw = (double *)B.bw.ensure(sizeof(double) * (size_t)grid * bw_per);
+            CK(cudaMemcpyAsync(d_runs, hr.data(), sizeof(IntegrateArgs) * hr.size(), cudaMemcpyHostToDevice, B.st));
+            CK(cudaMemcpyAsync(d_items, hi.data(), sizeof(int2) * hi.size(), cudaMemcpyHostToDevice, B.st));
+            CK(cudaMemsetAsync(d_counter, 0, sizeof(int), B.st));
+            CK(cudaEventRecord(B.t0, B.st));
+            CK(launch_integrate_lanes_multi(kv.first, d_runs, d_items, (int)hi.size(), d_counter, mn, grid, d_hist,
+                                            hist_per, d_bw, bw_per, B.st));
+            CK(cudaEventRecord(B.t1, B.st));
+            CK(cudaEventSynchronize(B.t1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, B.t0, B.t1));
+            B.kernel_ms += ms;
+            ++B.launches;
+        }
+        CK(cudaEventRecord(B.done, B.st));
+    } catch (const Err &e) {
+        R.err = e.what();
+    }
+    R.launched = true;
+    R.cv.notify_all();
+}
+
+static void release_batch_launch() {
+    if (!g_batch_launch) return;
+    BatchLaunch &B = *g_batch_launch;
+    cudaStreamSynchronize(B.st);
+    for (DBuf *b : {&B.runs, &B.items, &B.counter, &B.hist, &B.bw}) b->release();
+    cudaEventDestroy(B.done);
+    cudaEventDestroy(B.t0);
+    cudaEventDestroy(B.t1);
+    cudaStreamDestroy(B.st);
+    delete g_batch_launch;
+    g_batch_launch = nullptr;
+}
+
+// A group of the round takes part in the combined launch; returns once it is enqueued.
+static void round_join(BatchRound &R, const IntegrateArgs &ia, int model, cudaEvent_t ready) {
+    std::unique_lock<std::mutex> lk(R.mu);
+    R.joins.push_back({ia, model, ready});
+    if (++R.resolved == R.expected) round_launch(R);
+    else R.cv.wait(lk, [&] { return R.launched; });
+    if (!R.err.empty()) throw Err(CBNM_ERR_CUDA, R.err);
+}
+
+// A group of the round that does not take part (another integrator, or an error).
+static void round_decline(BatchRound &R) {
+    std::unique_lock<std::mutex> lk(R.mu);
+    if (++R.resolved == R.expected) round_launch(R);
 }
 
 // ---------------------------------------------------------------- FP32 integrator variants
@@ -824,6 +948,10 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (!force_simt || tan_bold) && !use_tc)
                                           : (variant == V_LANES || variant == V_LANES512);
     const int lanes_threads = variant == V_LANES512 ? 512 : 1024;
+    if (t_round && !t_round_resolved && !(use_lanes && lanes_threads == 1024 && !tan_bold && g_batch_launch)) {
+        t_round_resolved = true;  // this group runs its own integrator: the round need not wait for it
+        round_decline(*t_round);
+    }
     if (has_delay) {
         S.d_delay.ensure(sizeof(int) * h_delay.size());
         CK(cudaMemcpyAsync(S.d_delay.p, h_delay.data(), sizeof(int) * h_delay.size(), cudaMemcpyHostToDevice, S.st));
@@ -1082,12 +1210,24 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         ia.ln_params = (float *)S.d_ln_params.ensure(sizeof(float) * (size_t)ia.ln_n_groups * n * md.n_regional * G);
         ia.ln_hist_per_cta = (long long)max_slots * n * G * (tan_bold ? 2 : 1);  // (x, dx/dG) pairs with the tangent
         ia.tan_bold = tan_bold;
-        ia.ln_hist = (float *)S.d_ln_hist.ensure(sizeof(float) * (size_t)ia.ln_grid * ia.ln_hist_per_cta);
-        ia.ln_bw = (double *)S.d_ln_bw.ensure(sizeof(double) * (size_t)ia.ln_grid * n * (tan_bold ? 8 : 4) * G);
-        CK(cudaStreamSynchronize(S.st));
-        CK(cudaEventRecord(S.ev[1], S.st));
-        CK(launch_integrate_lanes(md.id, ia, S.st));
-        launches += 2;  // parameter layout + integrator
+        const bool join = t_round && !t_round_resolved && !tan_bold && lanes_threads == 1024 && g_batch_launch;
+        if (join) {  // one launch for the lane groups of the batch round
+            CK(cudaStreamSynchronize(S.st));
+            CK(cudaEventRecord(S.ev[1], S.st));
+            CK(launch_integrate_lanes_params(md.id, ia, S.st));
+            CK(cudaEventRecord(S.ev[5], S.st));
+            t_round_resolved = true;
+            round_join(*t_round, ia, md.id, S.ev[5]);
+            CK(cudaStreamWaitEvent(S.st, g_batch_launch->done, 0));
+            launches += 1;  // parameter layout; the combined integrator launch is counted by the batch
+        } else {
+            ia.ln_hist = (float *)S.d_ln_hist.ensure(sizeof(float) * (size_t)ia.ln_grid * ia.ln_hist_per_cta);
+            ia.ln_bw = (double *)S.d_ln_bw.ensure(sizeof(double) * (size_t)ia.ln_grid * n * (tan_bold ? 8 : 4) * G);
+            CK(cudaStreamSynchronize(S.st));
+            CK(cudaEventRecord(S.ev[1], S.st));
+            CK(launch_integrate_lanes(md.id, ia, S.st));
+            launches += 2;  // parameter layout + integrator
+        }
     } else if (c.fp32) {
         CK(cudaStreamSynchronize(S.st));
         CK(cudaEventRecord(S.ev[1], S.st));
@@ -1479,13 +1619,36 @@ int cbnm_run_batch(const cbnm_run_args *args, cbnm_outputs *outs, int n_groups, 
         std::vector<std::string> errs(n_groups);
         std::atomic<int> launches{0};
         std::atomic<long long> h2d{0}, d2h{0};
+        // the lane groups of each round of K groups share one launch (CBNM_BATCH_LAUNCH=streams:
+        // every group launches its own kernel on its own stream)
+        const char *bl = std::getenv("CBNM_BATCH_LAUNCH");
+        const bool combined = !(bl && std::string(bl) == "streams");
+        const int n_rounds = (n_groups + K - 1) / K;
+        std::vector<BatchRound> rounds(n_rounds);
+        for (int r = 0; r < n_rounds; ++r) rounds[r].expected = std::min(K, n_groups - r * K);
+        if (combined) {
+            if (!g_batch_launch) {
+                g_batch_launch = new BatchLaunch();
+                CK(cudaStreamCreateWithFlags(&g_batch_launch->st, cudaStreamNonBlocking));
+                CK(cudaEventCreateWithFlags(&g_batch_launch->done, cudaEventDisableTiming));
+                CK(cudaEventCreate(&g_batch_launch->t0));
+                CK(cudaEventCreate(&g_batch_launch->t1));
+            }
+            g_batch_launch->kernel_ms = 0.0f;
+            g_batch_launch->launches = 0;
+            g_batch_launch->host_runs.clear();
+            g_batch_launch->host_items.clear();
+        }
         const double t0 = now_s();
         auto worker = [&](int w) {
             const cudaError_t e = cudaSetDevice(dev);
             for (int g = w; g < n_groups; g += K) {
+                t_round = combined ? &rounds[g / K] : nullptr;
+                t_round_resolved = false;
                 if (e != cudaSuccess) {
                     codes[g] = CBNM_ERR_CUDA;
                     errs[g] = std::string("CUDA Error: ") + cudaGetErrorString(e);
+                    if (t_round) round_decline(*t_round);
                     continue;
                 }
                 try {
@@ -1501,6 +1664,8 @@ int cbnm_run_batch(const cbnm_run_args *args, cbnm_outputs *outs, int n_groups, 
                     codes[g] = CBNM_ERR_CONFIG;
                     errs[g] = x.what();
                 }
+                if (t_round && !t_round_resolved) round_decline(*t_round);
+                t_round = nullptr;
             }
         };
         std::vector<std::thread> pool;
@@ -1513,6 +1678,10 @@ int cbnm_run_batch(const cbnm_run_args *args, cbnm_outputs *outs, int n_groups, 
             tm.fc_ms = std::max(tm.fc_ms, g_batch[w]->timing.fc_ms);
         }
         tm.kernel_launches = launches.load();
+        if (combined) {  // the combined integrator launches: their device time and count
+            tm.kernel_launches += g_batch_launch->launches;
+            if (g_batch_launch->launches) tm.integrate_ms = std::max(tm.integrate_ms, (double)g_batch_launch->kernel_ms);
+        }
         tm.h2d_bytes = h2d.load();
         tm.d2h_bytes = d2h.load();
         g_last_timing = tm;
