@@ -42,9 +42,14 @@ N_SIMS = 32768
 NODES = 100
 DURATION_S = 60
 # dram__bytes_read.sum + dram__bytes_write.sum of one integrator launch of the default
-# workload (9,673 MB + 4,926 MB), measured by ncu with those one-pass metrics on the
-# full-size run (python bench.py --steps 1 --warmup 0 --skip-fp64 --skip-cpu)
-TRAFFIC_DEFAULT_WORKLOAD = 14.5994e9
+# workload, from an ncu capture of one launch on a reduced case scaled by the
+# simulated node-steps (profiles/ names the capture); None until measured
+TRAFFIC_DEFAULT_WORKLOAD = None
+TRAFFIC_SOURCE = None
+# FP32 flops of one rWW node update (rww.cpp:194-232): I_E 8, I_I 4, the two affine
+# rate arguments 4, the two rates (without their exp) 6, dS_E 8, dS_I 6, the two
+# state additions 2
+RWW_FP32_FLOPS = 38
 WORKLOAD = f"rWW {NODES} nodes, {N_SIMS} sims, {DURATION_S} s, dt 0.1 ms, TR 1 s, FC+FCD w10/s2"
 METRIC = "rWW sims x sim-s per wall-s (100 nodes, 32k sims)"
 UNIT = "sims*sim-s/s"
@@ -194,6 +199,7 @@ def run_ours(opts, rank, world, local_rank):
     e1.record(st)
     barrier()
     ck = clocks.stop()
+    integrator = core.last_integrator()
     ms = max_over_ranks(e0.elapsed_time(e1) / opts.steps)
     value = world * n_sims * opts.duration / (ms / 1e3)
 
@@ -247,27 +253,41 @@ def run_ours(opts, rank, world, local_rank):
                 "fp32_same_subset_fic_e2e": n64 * opts.duration / t_fic,
                 "sims": n64, "unit": UNIT}
 
-    # roofline of the dominant kernel (the integrator): coupling on the tensor pipe
+    # roofline of the dominant kernel (the integrator).  Its binding resource is the
+    # FP32 / MUFU node update (ncu: profiles/), so the bound reported is FP32 FLOP/s of
+    # the update against this GPU's measured FMA throughput; the coupling GEMM's
+    # tensor-pipe fraction is reported beside it.
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     peak_tf = peaks.get("bf16_tflops_sustained") or 1400.0
+    f1, f2 = C.c_double(), C.c_double()
+    check(L.cbnm_measure_fp32_peak(C.byref(f1), C.byref(f2)))
+    fp32_peak = max(f1.value, f2.value)
     node_steps = n_sims * NODES * (opts.duration * 1000 / 0.1)
     integ = float(np.mean(integ_ms)) / 1e3
     useful = 2.0 * NODES * node_steps  # coupling flops (2 n per node-step)
     issued = 3 * 2.0 * 128 * (((NODES + 15) // 16) * 16) * (n_sims * 1.0) * (opts.duration * 1e4)  # BF16x3 MMA work
+    fp32_flops = RWW_FP32_FLOPS * node_steps
     traffic, traffic_src = opts.traffic, "--traffic" if opts.traffic is not None else None
     if traffic is None and n_sims == N_SIMS and opts.duration == DURATION_S and opts.precision == "fp32":
-        traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, "ncu one-pass capture of this full-size workload"
-    roof = {"bound": "tensor", "achieved": useful / integ / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
-            "frac": useful / integ / 1e12 / peak_tf,
-            "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else "fallback",
-            "mma_issued_tflops": issued / integ / 1e12,
-            "traffic": traffic, "traffic_source": traffic_src, "kernel": "k_integrate_tc<RWW32>",
-            "kernel_ms": integ * 1e3,
-            "note": "integrator is bound by the FP32/MUFU elementwise update, not the tensor pipe; see profiles/"}
+        traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, TRAFFIC_SOURCE
+    roof = {"bound": "fp32", "achieved": fp32_flops / integ / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": fp32_flops / integ / 1e12 / fp32_peak,
+            "peak_source": f"measured on this GPU by cbnm_measure_fp32_peak (FFMA {f1.value:.1f}, "
+                           f"FFMA2 {f2.value:.1f} TFLOP/s)",
+            "work": f"{RWW_FP32_FLOPS} FP32 flops per node-step (rWW update), {node_steps:.3e} node-steps",
+            "tensor": {"achieved": useful / integ / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
+                       "frac": useful / integ / 1e12 / peak_tf,
+                       "peak_source": ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks
+                                       else "fallback"),
+                       "mma_issued_tflops": issued / integ / 1e12},
+            "traffic": traffic, "traffic_source": traffic_src,
+            "algorithmic_bytes": N_SIMS * NODES * DURATION_S * 8.0 if n_sims == N_SIMS else None,
+            "kernel": "k_integrate_pp<RWW32>", "kernel_ms": integ * 1e3,
+            "note": "per-pipe utilisation of this kernel: profiles/ (ncu)"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": opts.steps,
@@ -281,6 +301,7 @@ def run_ours(opts, rank, world, local_rank):
                 "d2h_bytes_per_step": d2h // e2e_steps, "includes": "H2D params/SC, kernels, D2H outputs, GOF"},
         "gpu_launches": launches,
         "kernel_ms": {"integrate": float(np.mean(integ_ms)), "fc_fcd": float(np.mean(fc_ms))},
+        "integrator": integrator,
         "fp64_path": fp64,
         "error_vs_fp64": line_errors,
         "roofline": roof,

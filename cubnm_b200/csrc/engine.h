@@ -187,6 +187,8 @@ struct FitLossArgs {
     double *fc, *wfc, *fcd, *wstat, *stats, *g_fc, *g_fcd, *g_wfc;
 };
 cudaError_t launch_fit_loss(const FitLossArgs &a, cudaStream_t st, int *launches);
+// FP32 FMA throughput of the current device (peak.cu), TFLOP/s, scalar and packed.
+cudaError_t measure_fp32_peak(double *ffma_tflops, double *ffma2_tflops);
 size_t fit_loss_sort_smem(int n_window_pairs);
 
 // Adjoint (reverse-mode) pass of the FP32 rWW integrator + FP64 Balloon-Windkessel

@@ -1705,6 +1705,13 @@ const char *cbnm_last_error(void) { return g_err.c_str(); }
 
 const char *cbnm_last_integrator(void) { return t_last_variant.c_str(); }
 
+int cbnm_measure_fp32_peak(double *ffma_tflops, double *ffma2_tflops) {
+    return guarded([&] {
+        if (!ffma_tflops || !ffma2_tflops) throw Err(CBNM_ERR_ARG, "null output");
+        CK(measure_fp32_peak(ffma_tflops, ffma2_tflops));
+    });
+}
+
 int cbnm_tune_reset(void) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tuned.clear();

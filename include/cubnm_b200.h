@@ -192,6 +192,12 @@ const char *cbnm_last_error(void);
  * "simt" (one CTA per simulation).  No reference counterpart (diagnostic). */
 const char *cbnm_last_integrator(void);
 
+/* FP32 fused-multiply-add throughput of the current device in TFLOP/s (two flops
+ * a lane per FMA), scalar and packed two-wide: the measured denominator of the
+ * integrators' FP32 roofline.  Takes about a quarter of a second.  No reference
+ * counterpart (diagnostic). */
+int cbnm_measure_fp32_peak(double *ffma_tflops, double *ffma2_tflops);
+
 /* Forgets the autotuner's choices (model_config "autotune" = "1" or
  * CBNM_AUTOTUNE=1: the first run of each workload -- model, nodes, largest
  * delay, number of SCs -- times a short probe of every applicable FP32
