@@ -89,6 +89,7 @@ struct IntegrateArgs {
     int *status;                 // device status word (0 = ok)
     double *bw_scratch;          // two-tile kernel: per-CTA Balloon-Windkessel state (pp_bw_scratch_bytes)
     int pp_grid;                 // two-tile kernel: CTAs launched (the scratch holds this many)
+    int pp_ws;                   // two-tile kernel: 1 = warp-specialised halves (1024 threads), 0 = 544 threads
     // lane kernel (integrate_lanes.cu): groups of 16 simulations sharing SC and delay table
     const int *ln_groups;        // [ln_n_groups][3 + 16] = SC index, delay table, max delay (1 without delays), simulations
     int ln_n_groups;

@@ -41,6 +41,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <cuda/atomic>
 #include "engine.h"
 #include "tc_common.cuh"
 
@@ -61,6 +62,7 @@ struct PPSmem {
     uint64_t mbar_x[2];     // B operand of half h written (PP_UPD arrivals per step)
     uint32_t tmem_base;
     int abort;
+    unsigned int arrived[2];  // warp-specialised form: warps of half h done writing its B operand this step
 };
 
 __host__ __device__ constexpr size_t pp_b_bytes(int KP) { return (size_t)KP * PP_TN * 2; }
@@ -92,21 +94,28 @@ __device__ __noinline__ void pp_states_out(const IntegrateArgs &a, const int *wd
     }
 }
 
-template <class M>
-__global__ void __maxnreg__(120)
-    k_integrate_pp(const __grid_constant__ IntegrateArgs a, const int *work, int n_work, int KP, int use_sacc) {
+// WS = false: warps 0-15 update both halves, warp 16 issues the MMAs (544 threads).
+// WS = true: warps 0-15 update half 0 and warps 16-31 half 1 (1024 threads), so the
+// two halves' updates can run at the same time; the last warp of a half to finish
+// writing its B operand issues that half's MMAs (counted in shared memory).
+template <class M, bool WS>
+__device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work, int n_work, int KP, int use_sacc) {
     static_assert(M::PAIR && M::NP <= 5, "parameters of 64 simulations must fit beside the SC in TMEM");
+    constexpr int NUPD = WS ? 1024 : PP_UPD;      // update threads
+    constexpr int NH = WS ? 1 : 2;                // halves a thread updates
+    constexpr int NPAIR = NH * PP_SPT / 2;        // simulation pairs a thread updates
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const int n = a.nodes;
     const size_t bb = pp_b_bytes(KP);
     float *zbuf = reinterpret_cast<float *>(smem_raw + 4 * bb);
-    float *sacc = zbuf + 2 * PP_SPT * PP_UPD;
+    float *sacc = zbuf + NH * PP_SPT * NUPD;
     PPSmem *sm = reinterpret_cast<PPSmem *>(reinterpret_cast<uint8_t *>(sacc) +
                                             (use_sacc ? pp_sacc_bytes(M::NOUT, n) : 0));
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const bool issuer_warp = warp == PP_UPD / 32;
+    const bool issuer_warp = !WS && warp == PP_UPD / 32;
+    const int h_own = WS ? (warp >> 4) : 0;  // the half of a warp-specialised thread
     const int quarter = warp & 3;
     const int g = (warp >> 2) & 3;           // simulations 8 g .. 8 g + 7 of each half
     const int j = quarter * 32 + lane;       // node = TMEM lane
@@ -121,6 +130,7 @@ __global__ void __maxnreg__(120)
         for (int h = 0; h < 2; ++h) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm->mbar_mma[h])), "r"(1));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm->mbar_x[h])), "r"(PP_UPD));
+            sm->arrived[h] = 0u;
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         sm->abort = 0;
@@ -148,12 +158,13 @@ __global__ void __maxnreg__(120)
         const int *wd = work + (size_t)w * (1 + PP_SIMS);
         const int sc_idx = wd[0];
         const bool live[2] = {wd[1] >= 0, wd[1 + PP_TN] >= 0};
-        float2 s2[2][PP_SPT / 2][M::NS];    // node state of the thread's pairs, both halves
+        float2 s2[NH][PP_SPT / 2][M::NS];   // node state of the thread's pairs
 
         if (!issuer_warp) {
             // ---- parameters -> TMEM; initial state; SC^T when the SC changes
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int hh = 0; hh < NH; ++hh) {
+                const int h = WS ? h_own : hh;
                 uint32_t pw[M::NP][PP_SPT];
 #pragma unroll
                 for (int pr = 0; pr < PP_SPT / 2; ++pr) {
@@ -181,13 +192,13 @@ __global__ void __maxnreg__(120)
                         pw[q][2 * pr + 1] = __float_as_uint(p2[q].y);
                     }
 #pragma unroll
-                    for (int q = 0; q < M::NS; ++q) s2[h][pr][q] = make_float2(sa[0][q], sa[1][q]);
+                    for (int q = 0; q < M::NS; ++q) s2[hh][pr][q] = make_float2(sa[0][q], sa[1][q]);
                 }
 #pragma unroll
                 for (int q = 0; q < M::NP; ++q) tmem_st8_nowait(t_lane + col_p + (h * M::NP + q) * PP_TN + g * PP_SPT, pw[q]);
             }
             tmem_wait_st();
-            if (sc_loaded != sc_idx && g == 0) {  // warpgroup 0 writes SC^T (each warp its lane quarter)
+            if (sc_loaded != sc_idx && g == 0 && h_own == 0) {  // warpgroup 0 writes SC^T (each warp its lane quarter)
                 const float *SC = a.sc_f32 + (size_t)sc_idx * n * n;
                 for (int c0 = 0; c0 < half_k; c0 += 8) {
                     uint32_t hw[8], lw[8];
@@ -202,11 +213,11 @@ __global__ void __maxnreg__(120)
                     tmem_st8(t_lane + PP_COL_A + half_k + c0, lw);
                 }
             }
-            // Balloon-Windkessel state x = 0, f = nu = q = 1 for the thread's 8 pairs
+            // Balloon-Windkessel state x = 0, f = nu = q = 1 for the thread's pairs
             if (act) {
 #pragma unroll
-                for (int p = 0; p < PP_PAIRS; ++p) {
-                    double2 *b = bws + (size_t)((p >> 2) * 16 + g * 4 + (p & 3)) * 4 * n + j;
+                for (int p = 0; p < NPAIR; ++p) {
+                    double2 *b = bws + (size_t)(((WS ? h_own : (p >> 2))) * 16 + g * 4 + (p & 3)) * 4 * n + j;
                     b[0] = make_double2(0.0, 0.0);
                     b[n] = make_double2(1.0, 1.0);
                     b[2 * n] = make_double2(1.0, 1.0);
@@ -215,8 +226,9 @@ __global__ void __maxnreg__(120)
             }
             if (a.ext_out && !a.states_ts && act) {  // state sums start at zero
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+                for (int hh = 0; hh < NH; ++hh)
                     for (int i = 0; i < PP_SPT; ++i) {
+                        const int h = WS ? h_own : hh;
                         const int slot = h * PP_TN + g * PP_SPT + i;
                         const int sim = wd[1 + slot];
                         for (int v = 0; v < M::NOUT; ++v) {
@@ -227,12 +239,13 @@ __global__ void __maxnreg__(120)
             }
         }
         // B operand of half h: rows of padded nodes are zero
-        auto write_x = [&](int h) {
+        auto write_x = [&](int hh) {
             if (j >= KP) return;
+            const int h = WS ? h_own : hh;
             uint32_t hw[PP_SPT / 2], lw[PP_SPT / 2];
 #pragma unroll
             for (int pr = 0; pr < PP_SPT / 2; ++pr) {
-                const float2 x = act ? s2[h][pr][M::CV] : make_float2(0.0f, 0.0f);
+                const float2 x = act ? s2[hh][pr][M::CV] : make_float2(0.0f, 0.0f);
                 split_bf16x2(x.x, x.y, hw[pr], lw[pr]);
             }
             const int s0 = g * PP_SPT;
@@ -240,20 +253,50 @@ __global__ void __maxnreg__(120)
             *reinterpret_cast<uint4 *>(smem_raw + (2 * h) * bb + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
             *reinterpret_cast<uint4 *>(smem_raw + (2 * h + 1) * bb + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
         };
+        // the 21 MMAs of one step of half h (BF16x3, 3 per K chunk of 16), committed to mbar_mma[h]
+        auto issue = [&](int h) {
+            const uint32_t idesc = instr_desc(PP_TN);
+            const uint32_t bh = smem_u32(smem_raw + (2 * h) * bb), bl = smem_u32(smem_raw + (2 * h + 1) * bb);
+            const uint32_t d = tmem + h * PP_TN;
+            for (int kk = 0; kk < KP / 16; ++kk) {
+                const uint32_t tah = tmem + PP_COL_A + kk * 8, tal = tah + half_k;
+                const uint64_t dbh = smem_desc(bh + kk * 2 * PP_LBO, PP_LBO, 128);
+                const uint64_t dbl = smem_desc(bl + kk * 2 * PP_LBO, PP_LBO, 128);
+                mma_bf16_ts(d, tah, dbh, idesc, kk > 0 ? 1u : 0u);
+                mma_bf16_ts(d, tah, dbl, idesc, 1u);
+                mma_bf16_ts(d, tal, dbh, idesc, 1u);
+            }
+            mma_commit(smem_u32(&sm->mbar_mma[h]));
+        };
+        // B operand of half h written: the last of its 16 warps issues the half's GEMM
+        auto arrive_ws = [&](int h) {
+            fence_proxy_async();
+            fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                cuda::atomic_ref<unsigned int, cuda::thread_scope_block> cnt(sm->arrived[h]);
+                if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == 15u) {
+                    cnt.store(0u, cuda::memory_order_relaxed);
+                    fence_after();
+                    issue(h);
+                }
+            }
+            __syncwarp();
+        };
         if (!issuer_warp) {
-            write_x(0);
-            write_x(1);
+#pragma unroll
+            for (int hh = 0; hh < NH; ++hh) write_x(hh);
             fence_proxy_async();
         }
         fence_before();
         __syncthreads();
         fence_after();
         sc_loaded = sc_idx;
+        if (WS && live[h_own] && tid == h_own * 512) issue(h_own);  // step 0 of each half
 
         if (issuer_warp) {
             // ---- MMA issue: GEMM k of half h once its B operand is written
             if (lane == 0) {
-                const uint32_t idesc = instr_desc(PP_TN);
                 bool stop = false;
                 for (int k = 0; k < steps && !stop; ++k) {
 #pragma unroll
@@ -269,17 +312,7 @@ __global__ void __maxnreg__(120)
                             if (*(volatile int *)&sm->abort) { stop = true; break; }
                         }
                         fence_after();
-                        const uint32_t bh = smem_u32(smem_raw + (2 * h) * bb), bl = smem_u32(smem_raw + (2 * h + 1) * bb);
-                        const uint32_t d = tmem + h * PP_TN;
-                        for (int kk = 0; kk < KP / 16; ++kk) {
-                            const uint32_t tah = tmem + PP_COL_A + kk * 8, tal = tah + half_k;
-                            const uint64_t dbh = smem_desc(bh + kk * 2 * PP_LBO, PP_LBO, 128);
-                            const uint64_t dbl = smem_desc(bl + kk * 2 * PP_LBO, PP_LBO, 128);
-                            mma_bf16_ts(d, tah, dbh, idesc, kk > 0 ? 1u : 0u);
-                            mma_bf16_ts(d, tah, dbl, idesc, 1u);
-                            mma_bf16_ts(d, tal, dbh, idesc, 1u);
-                        }
-                        mma_commit(smem_u32(&sm->mbar_mma[h]));
+                        issue(h);
                     }
                 }
             }
@@ -294,20 +327,21 @@ __global__ void __maxnreg__(120)
             bool aborted = false, pend = false, pend_tr = false;
             int pend_bi = 0;
             double2 bwx[4];  // Balloon-Windkessel state of the next pair, loaded ahead
-            const bool ahead = a.inner_it >= PP_PAIRS;   // one pair per inner step, loads one step ahead
-            auto bw_ptr = [&](int p) { return bws + (size_t)((p >> 2) * 16 + g * 4 + (p & 3)) * 4 * n + j; };
+            const bool ahead = a.inner_it >= NPAIR;   // one pair per inner step, loads one step ahead
+            auto half_of = [&](int p) { return WS ? h_own : (p >> 2); };
+            auto bw_ptr = [&](int p) { return bws + (size_t)(half_of(p) * 16 + g * 4 + (p & 3)) * 4 * n + j; };
             auto bw_load = [&](int p) {
-                if (!act || !live[p >> 2]) return;
+                if (!act || !live[half_of(p)]) return;
                 const double2 *b = bw_ptr(p);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) bwx[c] = __ldcg(b + (size_t)c * n);
             };
             // one bw step of pair p (inputs: z of the previous bw step), BOLD at TR
             auto bw_do = [&](int p) {
-                if (!act || !live[p >> 2]) return;
+                if (!act || !live[half_of(p)]) return;
                 double x[2] = {bwx[0].x, bwx[0].y}, f[2] = {bwx[1].x, bwx[1].y};
                 double nu[2] = {bwx[2].x, bwx[2].y}, q[2] = {bwx[3].x, bwx[3].y};
-                const float z0 = zbuf[(2 * p) * PP_UPD + tid], z1 = zbuf[(2 * p + 1) * PP_UPD + tid];
+                const float z0 = zbuf[(2 * p) * NUPD + tid], z1 = zbuf[(2 * p + 1) * NUPD + tid];
                 bw_step64x2(x, f, nu, q, (double)z0, (double)z1, bw);
                 double2 *b = bw_ptr(p);
                 __stcg(b, make_double2(x[0], x[1]));
@@ -317,7 +351,7 @@ __global__ void __maxnreg__(120)
                 if (pend_tr && pend_bi < a.bold_len) {  // no slot for a sample past bold_len
 #pragma unroll
                     for (int u = 0; u < 2; ++u) {
-                        const int sim = wd[1 + (p >> 2) * PP_TN + g * PP_SPT + 2 * (p & 3) + u];
+                        const int sim = wd[1 + half_of(p) * PP_TN + g * PP_SPT + 2 * (p & 3) + u];
                         if (sim >= 0)
                             a.bold[(size_t)sim * a.bold_len * n + (size_t)pend_bi * n + j] =
                                 bw.V0k1 * (1 - q[u]) + bw.V0k2 * (1 - q[u] / nu[u]) + bw.V0k3 * (1 - nu[u]);
@@ -345,7 +379,8 @@ __global__ void __maxnreg__(120)
                         if (M::NN > 1) nz1 = __ldg(nr + 1);
                     }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
+                    for (int hh = 0; hh < NH; ++hh) {
+                        const int h = WS ? h_own : hh;
                         if (!live[h]) continue;
                         const bool ok = mbar_wait(smem_u32(&sm->mbar_mma[h]), ph_mma[h]);
                         ph_mma[h] ^= 1u;
@@ -369,7 +404,7 @@ __global__ void __maxnreg__(120)
 #pragma unroll
                                 for (int q = 0; q < M::NP; ++q)
                                     p2[q] = make_float2(__uint_as_float(pw[q][0]), __uint_as_float(pw[q][1]));
-                                PairStep<M>::step(s2[h][pr], p2, make_float2(__uint_as_float(acc[0]), __uint_as_float(acc[1])),
+                                PairStep<M>::step(s2[hh][pr], p2, make_float2(__uint_as_float(acc[0]), __uint_as_float(acc[1])),
                                                   n0, n1, K, o);
                                 if (out_now)
                                     pp_states_out<M::NOUT>(a, wd, sacc, use_sacc, o, h * PP_TN + g * PP_SPT + 2 * pr, j,
@@ -377,10 +412,14 @@ __global__ void __maxnreg__(120)
                             }
                         }
                         if (!last_step) {
-                            write_x(h);
-                            fence_proxy_async();
-                            fence_before();
-                            mbar_arrive(smem_u32(&sm->mbar_x[h]));
+                            write_x(hh);
+                            if constexpr (WS) {
+                                arrive_ws(h);
+                            } else {
+                                fence_proxy_async();
+                                fence_before();
+                                mbar_arrive(smem_u32(&sm->mbar_x[h]));
+                            }
                         }
                     }
                     if (aborted) break;
@@ -389,12 +428,12 @@ __global__ void __maxnreg__(120)
                     // a bw step has fewer inner steps than the thread has pairs
                     if (pend) {
                         if (ahead) {
-                            if (inner < PP_PAIRS) {
+                            if (inner < NPAIR) {
                                 bw_do(inner);
-                                if (inner + 1 < PP_PAIRS) bw_load(inner + 1);
+                                if (inner + 1 < NPAIR) bw_load(inner + 1);
                             }
                         } else if (inner == 0) {
-                            for (int p = 0; p < PP_PAIRS; ++p) {
+                            for (int p = 0; p < NPAIR; ++p) {
                                 bw_load(p);
                                 bw_do(p);
                             }
@@ -404,11 +443,11 @@ __global__ void __maxnreg__(120)
                 if (aborted) break;
                 // this bw step's Balloon-Windkessel inputs; the updates run during the next bw step
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+                for (int hh = 0; hh < NH; ++hh)
 #pragma unroll
                     for (int pr = 0; pr < PP_SPT / 2; ++pr) {
-                        zbuf[(h * PP_SPT + 2 * pr) * PP_UPD + tid] = s2[h][pr][M::BV].x;
-                        zbuf[(h * PP_SPT + 2 * pr + 1) * PP_UPD + tid] = s2[h][pr][M::BV].y;
+                        zbuf[(hh * PP_SPT + 2 * pr) * NUPD + tid] = s2[hh][pr][M::BV].x;
+                        zbuf[(hh * PP_SPT + 2 * pr + 1) * NUPD + tid] = s2[hh][pr][M::BV].y;
                     }
                 pend = true;
                 pend_tr = ((bw_i + 1) % a.bold_tr_iters == 0);
@@ -421,7 +460,7 @@ __global__ void __maxnreg__(120)
                 if (ahead) bw_load(0);
             }
             if (pend && !aborted) {  // the last bw step
-                for (int p = 0; p < PP_PAIRS; ++p) {
+                for (int p = 0; p < NPAIR; ++p) {
                     if (p > 0 || !ahead) bw_load(p);
                     bw_do(p);
                 }
@@ -429,8 +468,9 @@ __global__ void __maxnreg__(120)
             if (a.ext_out && !a.states_ts && act && !aborted) {
                 const int pts = states_i - a.n_states_samples_remove;
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+                for (int hh = 0; hh < NH; ++hh)
                     for (int i = 0; i < PP_SPT; ++i) {
+                        const int h = WS ? h_own : hh;
                         const int slot = h * PP_TN + g * PP_SPT + i;
                         const int sim = wd[1 + slot];
                         if (sim < 0) continue;
@@ -454,6 +494,18 @@ __global__ void __maxnreg__(120)
 }
 
 template <class M>
+__global__ void __maxnreg__(120)
+    k_integrate_pp(const __grid_constant__ IntegrateArgs a, const int *work, int n_work, int KP, int use_sacc) {
+    pp_body<M, false>(a, work, n_work, KP, use_sacc);
+}
+
+template <class M>
+__global__ void __launch_bounds__(1024, 1)
+    k_integrate_pp_ws(const __grid_constant__ IntegrateArgs a, const int *work, int n_work, int KP, int use_sacc) {
+    pp_body<M, true>(a, work, n_work, KP, use_sacc);
+}
+
+template <class M>
 size_t pp_smem(int KP, int n, int *use_sacc) {
     const size_t base = 4 * pp_b_bytes(KP) + pp_z_bytes() + sizeof(PPSmem) + 64;
     const size_t with = base + pp_sacc_bytes(M::NOUT, n);
@@ -466,10 +518,16 @@ cudaError_t launch_pp(const IntegrateArgs &a, cudaStream_t st) {
     const int KP = ((a.nodes + 15) / 16) * 16;
     int use_sacc = 0;
     const size_t smem = pp_smem<M>(KP, a.nodes, &use_sacc);
-    cudaError_t e = cudaFuncSetAttribute(k_integrate_pp<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     const int grid = std::min(a.n_tiles, a.pp_grid);
-    k_integrate_pp<M><<<grid, PP_THREADS, smem, st>>>(a, a.tiles, a.n_tiles, KP, use_sacc);
+    if (a.pp_ws) {
+        cudaError_t e = cudaFuncSetAttribute(k_integrate_pp_ws<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_integrate_pp_ws<M><<<grid, 1024, smem, st>>>(a, a.tiles, a.n_tiles, KP, use_sacc);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(k_integrate_pp<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_integrate_pp<M><<<grid, PP_THREADS, smem, st>>>(a, a.tiles, a.n_tiles, KP, use_sacc);
+    }
     return cudaGetLastError();
 }
 

@@ -661,8 +661,8 @@ static void round_decline(BatchRound &R) {
 // CBNM_AUTOTUNE=1) the first run of each workload key times a short probe of
 // every applicable variant on a slice of the batch and keeps the fastest for the
 // process (and in CBNM_TUNE_FILE when set, one "key variant" line each).
-enum Variant { V_DEFAULT = 0, V_PP, V_V5, V_LANES, V_LANES512, V_SIMT, V_COUNT };
-static const char *const kVariantName[V_COUNT] = {"default", "tc2", "tc1", "lanes", "lanes512", "simt"};
+enum Variant { V_DEFAULT = 0, V_PP, V_V5, V_LANES, V_LANES512, V_SIMT, V_PPWS, V_COUNT };
+static const char *const kVariantName[V_COUNT] = {"default", "tc2", "tc1", "lanes", "lanes512", "simt", "tc2ws"};
 static thread_local int t_force_variant = V_DEFAULT;  // set while a probe runs
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tuned;
@@ -926,7 +926,10 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     if (variant == V_DEFAULT && !tan_bold && c.fp32 && !force_simt && !device_io &&
         (c.autotune || (std::getenv("CBNM_AUTOTUNE") && std::string(std::getenv("CBNM_AUTOTUNE")) == "1"))) {
         std::vector<int> cands;
-        if (tc_ok && pp_supported(md.id, n, has_delay)) cands.push_back(V_PP);
+        if (tc_ok && pp_supported(md.id, n, has_delay)) {
+            cands.push_back(V_PP);
+            cands.push_back(V_PPWS);
+        }
         if (tc_ok) cands.push_back(V_V5);
         if (lanes_ok) cands.push_back(V_LANES);
         if (lanes_ok && n <= 128) cands.push_back(V_LANES512);
@@ -938,13 +941,15 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     }
     if (variant != V_DEFAULT) {  // a forced or tuned variant must apply to this run
         const bool ok = c.fp32 && !tan_bold &&
-                        ((variant == V_PP && tc_ok && pp_supported(md.id, n, has_delay)) || (variant == V_V5 && tc_ok) ||
+                        (((variant == V_PP || variant == V_PPWS) && tc_ok && pp_supported(md.id, n, has_delay)) ||
+                         (variant == V_V5 && tc_ok) ||
                          (variant == V_LANES && lanes_ok) || (variant == V_LANES512 && lanes_ok && n <= 128) ||
                          variant == V_SIMT);
         if (!ok) throw Err(CBNM_ERR_UNSUPPORTED, std::string("integrator variant ") + kVariantName[variant] +
                                                      " does not apply to this run");
     }
-    const bool use_tc = variant == V_DEFAULT ? (!tan_bold && !force_simt && tc_ok) : (variant == V_PP || variant == V_V5);
+    const bool use_tc = variant == V_DEFAULT ? (!tan_bold && !force_simt && tc_ok)
+                                             : (variant == V_PP || variant == V_PPWS || variant == V_V5);
     bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (!force_simt || tan_bold) && !use_tc)
                                           : (variant == V_LANES || variant == V_LANES512);
     const int lanes_threads = variant == V_LANES512 ? 512 : 1024;
@@ -1129,7 +1134,10 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     // single-tile one
     const char *tc_kind = std::getenv("CBNM_FP32_TC");
     const bool use_pp = use_tc && pp_supported(md.id, n, has_delay) &&
-                        (variant == V_DEFAULT ? !(tc_kind && std::string(tc_kind) == "v5") : variant == V_PP);
+                        (variant == V_DEFAULT ? !(tc_kind && std::string(tc_kind) == "v5")
+                                              : (variant == V_PP || variant == V_PPWS));
+    // the warp-specialised two-tile form: CBNM_FP32_TC=ws, or the tuned variant
+    const bool pp_ws = use_pp && (variant == V_DEFAULT ? (tc_kind && std::string(tc_kind) == "ws") : variant == V_PPWS);
     if (use_tc) {
         // tiles of simulations that share one SC
         const int TN = use_pp ? 32 : fp32_tile_for(n);
@@ -1157,6 +1165,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         }
         ia.n_tiles = (int)(tiles.size() / (TN + 1));
         if (use_pp) tiles = pair_tiles(tiles, ia.n_tiles, sm_count(), &ia.n_tiles, &ia.pp_grid);
+        ia.pp_ws = pp_ws ? 1 : 0;
         S.d_tiles.ensure(sizeof(int) * tiles.size());
         CK(cudaMemcpyAsync(S.d_tiles.p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, S.st));
         ia.tiles = S.d_tiles.as<int>();
@@ -1237,7 +1246,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         CK(launch_integrate_fp64(md.id, ia, S.st));
         ++launches;
     }
-    t_last_variant = !c.fp32 ? "fp64" : use_pp ? "tc2" : use_tc ? "tc1" : use_lanes ? (lanes_threads == 512 ? "lanes512" : "lanes") : "simt";
+    t_last_variant = !c.fp32 ? "fp64" : use_pp ? (pp_ws ? "tc2ws" : "tc2") : use_tc ? "tc1" : use_lanes ? (lanes_threads == 512 ? "lanes512" : "lanes") : "simt";
     CK(cudaEventRecord(S.ev[2], S.st));
     if (!device_io) {  // the integrator runs asynchronously: map the host output pages meanwhile
         prefault_host(o->sim_bold, sizeof(double) * bold_n);

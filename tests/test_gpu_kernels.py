@@ -58,12 +58,20 @@ def test_two_tile_kernel_matches_single_tile_and_fp64(N, monkeypatch):
                                 bold_remove_s=4)
     o64 = core.run_simulations(*_with(args, precision="fp64"))
     pp = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == "tc2"
+    monkeypatch.setenv("CBNM_FP32_TC", "ws")
+    ws = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == "tc2ws"
     monkeypatch.setenv("CBNM_FP32_TC", "v5")
     v5 = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == "tc1"
     monkeypatch.delenv("CBNM_FP32_TC")
     assert np.isfinite(pp["sim_bold"]).all()
     _bounds(o64, pp, nodes, 16, 4, 2)
     _bounds(o64, v5, nodes, 16, 4, 2)
+    # the two two-tile forms run the same arithmetic in the same order
+    np.testing.assert_array_equal(ws["sim_bold"], pp["sim_bold"])
+    np.testing.assert_array_equal(ws["_sim_states"], pp["_sim_states"])
     assert np.abs(pp["sim_bold"] - v5["sim_bold"]).max() < 1e-4
     np.testing.assert_allclose(pp["_sim_states"], v5["_sim_states"], rtol=1e-3, atol=1e-4)
 
