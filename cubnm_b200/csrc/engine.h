@@ -123,6 +123,7 @@ struct FcArgs {
     double *fcd;                 // [n_sims][n_window_pairs]
     double *wfc;                 // scratch [sim_count][n_windows][n_pairs]
     double *wstat;               // scratch [sim_count][n_windows][2] (mean, ssd)
+    int *status_fc;              // tensor-core FC: set to 1 if a bounded wait gave up
 };
 
 // Goodness of fit.
@@ -170,6 +171,9 @@ cudaError_t launch_rww_fic(const FicArgs &a, cudaStream_t st);
 // Normal noise from Philox4x32-10 + Box-Muller (noise.cu); out32 may be null.
 cudaError_t launch_philox_normals(uint32_t seed, double *out, float *out32, size_t count, cudaStream_t st);
 cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches);
+cudaError_t launch_fcd_only(const FcArgs &a, cudaStream_t st, int *launches);  // FCD of window FCs already in a.wfc
+// FC / window FCs on the tensor cores (fc_tc.cu; FP32 mode); pidx [nodes*nodes]: pair index of (i > j) or -1.
+cudaError_t launch_fc_tc(const FcArgs &a, const int *pidx, cudaStream_t st, int *launches);
 cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches);
 size_t gof_ks_smem_limit();
 

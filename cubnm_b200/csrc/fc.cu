@@ -141,4 +141,11 @@ cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches) {
     return e;
 }
 
+cudaError_t launch_fcd_only(const FcArgs &a, cudaStream_t st, int *launches) {
+    if (a.n_windows > 1024) return cudaErrorInvalidValue;
+    k_fcd<<<a.sim_count, FC_THREADS, 0, st>>>(a);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+}
+
 }  // namespace cbnm

@@ -140,6 +140,7 @@ struct Cfg {
     bool fp32 = false;
     bool philox = false;  // noise segment from Philox on the GPU instead of the host mt19937
     bool autotune = false;  // pick the FP32 integrator by timing short probe runs (model_config "autotune")
+    bool fc_tc = false;     // FP32 mode: FC / window FCs on the tensor cores (model_config "fc" = "tc")
     int nodes = 0, n_sims = 0, time_steps = 0, bold_tr = 0, states_sampling = 0, sim_seed = 0;
     double dt = 0.1, bw_dt = 0.001;
     int bold_len = 0, bold_tr_iters = 0, states_len = 0, states_sampling_iters = 0, bw_it = 0, inner_it = 0;
@@ -183,6 +184,10 @@ static void build_cfg(Cfg &c, const cbnm_run_args *a, const ModelDesc &md) {
             else throw Err(CBNM_ERR_CONFIG, "precision must be 'fp64' or 'fp32', got '" + v + "'");
         } else if (k == "autotune") {
             c.autotune = to_int(k, v) != 0;
+        } else if (k == "fc") {
+            if (v == "tc") c.fc_tc = true;
+            else if (v == "fp64") c.fc_tc = false;
+            else throw Err(CBNM_ERR_CONFIG, "fc must be 'fp64' or 'tc', got '" + v + "'");
         } else if (k == "noise") {
             if (v == "philox") c.philox = true;
             else if (v == "mt19937") c.philox = false;
@@ -323,6 +328,7 @@ struct Session {
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
     DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr, d_ln_groups, d_ln_params, d_ln_hist, d_ln_bw;
     DBuf fl_ec, fl_q, fl_win, fl_scr;  // fit loss
+    DBuf d_pidx;                       // tensor-core FC: pair index of (i, j)
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -376,7 +382,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw, &S.fl_ec, &S.fl_q, &S.fl_win, &S.fl_scr,
+                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw, &S.fl_ec, &S.fl_q, &S.fl_win, &S.fl_scr, &S.d_pidx,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -1291,10 +1297,22 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         fa.w_start = S.d_wstart.as<int>(); fa.w_end = S.d_wend.as<int>();
         fa.pair_i = S.d_pairs_i.as<int>(); fa.pair_j = S.d_pairs_j.as<int>();
         fa.bold = d_bold; fa.fc = d_fc; fa.fcd = d_fcd; fa.wfc = S.d_wfc.as<double>();
+        fa.status_fc = d_status;
+        // tensor-core FC in FP32 mode when asked for (model_config "fc" = "tc" or CBNM_FC=tc)
+        const char *fce = std::getenv("CBNM_FC");
+        const bool fc_tc = c.fp32 && (c.fc_tc || (fce && std::string(fce) == "tc"));
+        if (fc_tc) {
+            std::vector<int> pidx(nn, -1);
+            for (size_t q = 0; q < pi.size(); ++q) pidx[(size_t)pi[q] * n + pj[q]] = (int)q;
+            S.d_pidx.ensure(sizeof(int) * nn);
+            CK(cudaMemcpyAsync(S.d_pidx.p, pidx.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, S.st));
+            CK(cudaStreamSynchronize(S.st));
+        }
         for (int s0 = 0; s0 < N; s0 += chunk) {
             fa.sim_begin = s0;
             fa.sim_count = std::min(chunk, N - s0);
-            CK(launch_fc(fa, S.st, &launches));
+            if (fc_tc) CK(launch_fc_tc(fa, S.d_pidx.as<int>(), S.st, &launches));
+            else CK(launch_fc(fa, S.st, &launches));
         }
     }
     CK(cudaEventRecord(S.ev[3], S.st));
