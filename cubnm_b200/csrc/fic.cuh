@@ -16,10 +16,12 @@
 
 namespace cbnm {
 
-// Brent's method (Brent 1973; Numerical Recipes zbrent form) driven through
-// GSL's documented fsolver protocol: each iteration reports the bracket, the
-// caller stops when |hi-lo| < 1e-3 * min(|lo|,|hi|) (0 if the bracket holds 0),
-// at most 100 iterations, -1 on failure (rww_fic.cpp:62-102).
+// Brent's method (Brent 1973) with the iteration of GSL 2.7's brent fsolver
+// (gsl_root_fsolver_brent, the solver the reference calls in rww_fic.cpp:62-102)
+// step for step: the same interpolation / bisection switch, tolerance
+// 0.5 * DBL_EPSILON * |b| and bracket update, so that FIC parity holds.  Each
+// iteration reports the bracket; the caller stops when |hi-lo| < 1e-3 *
+// min(|lo|,|hi|) (0 if the bracket holds 0), at most 100 iterations, -1 on failure.
 template <class F>
 __host__ __device__ inline double brent_root(F f, double x_lo, double x_hi) {
     const double eps = 2.2204460492503131e-16;

@@ -19,8 +19,8 @@
  *                              src/ext/models/rww.cpp:54-71
  *
  * Third-party arithmetic restated here: GSL 2.7's Brent root bracketing
- * (gsl_root_fsolver_brent + gsl_root_test_interval, rww_fic.cpp:62-102), written
- * from Brent's published method in its Numerical-Recipes form (see brent_root);
+ * (gsl_root_fsolver_brent + gsl_root_test_interval, rww_fic.cpp:62-102), whose
+ * iteration brent_root follows step for step;
  * GSL's gsl_blas_ddot is a sequential dot product.  std::mt19937 and libstdc++'s
  * std::normal_distribution<double> produce the noise values as the reference
  * does (bnm.cpp:690-706); the node/time shuffles are restated (shuffle_ref).
@@ -357,8 +357,9 @@ struct ModelRWWEx {
 
 // ---------------------------------------------------------------- analytical FIC
 // Brent's method (R. P. Brent, "Algorithms for Minimization without
-// Derivatives", 1973, ch. 4; Numerical Recipes zbrent form) driven the way GSL's
-// documented fsolver interface drives it: every iteration reports the bracket
+// Derivatives", 1973, ch. 4) with the iteration of GSL 2.7's brent fsolver
+// (gsl_root_fsolver_brent, step for step, which FIC parity needs), driven the
+// way GSL's fsolver interface drives it: every iteration reports the bracket
 // [min(b,c), max(b,c)]; the caller stops when
 //   |hi - lo| < epsabs + epsrel * min(|lo|,|hi|)   (min -> 0 if 0 is inside)
 // with epsabs = 0, epsrel = 1e-3 and at most 100 iterations (rww_fic.cpp:62-102).
