@@ -25,8 +25,8 @@
 //    read per pair each step; the FP64 Balloon-Windkessel state (x, f, nu, q)
 //    lives in a per-CTA global scratch that stays in L2 (2 KB per node for the 64
 //    simulations), updated once per bw step for one simulation pair per inner
-//    step (after both halves' updates, while the next GEMMs run), its loads
-//    issued one inner step ahead.  The time-averaged states are
+//    step (after the halves' updates, while the next GEMMs run), staggered
+//    between warpgroups so that their loads spread over the bw step.  The time-averaged states are
 //    accumulated in shared memory (FP32) and written once per simulation.
 //  * Every wait is bounded (about 2 s); on timeout the CTA records a status,
 //    leaves its loops, frees its TMEM and returns.
@@ -326,8 +326,8 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
             float nz1 = (act && M::NN > 1) ? __ldg(nrow + 1) : 0.0f;
             bool aborted = false, pend = false, pend_tr = false;
             int pend_bi = 0;
-            double2 bwx[4];  // Balloon-Windkessel state of the next pair, loaded ahead
-            const bool ahead = a.inner_it >= NPAIR;   // one pair per inner step, loads one step ahead
+            double2 bwx[4];  // Balloon-Windkessel state of the pair being updated
+            const int stagger = (2 * g + (WS ? 5 * h_own : 0)) % a.inner_it;
             auto half_of = [&](int p) { return WS ? h_own : (p >> 2); };
             auto bw_ptr = [&](int p) { return bws + (size_t)(half_of(p) * 16 + g * 4 + (p & 3)) * 4 * n + j; };
             auto bw_load = [&](int p) {
@@ -423,20 +423,14 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
                         }
                     }
                     if (aborted) break;
-                    // Balloon-Windkessel work of the previous bw step: pair p at inner step p
-                    // (its state loaded one inner step ahead), or all pairs at inner step 0 when
-                    // a bw step has fewer inner steps than the thread has pairs
+                    // Balloon-Windkessel work of the previous bw step: pair p at inner step
+                    // (p + stagger) mod inner_it, the stagger differing between warpgroups so
+                    // that their L2 loads of the state spread over the bw step
                     if (pend) {
-                        if (ahead) {
-                            if (inner < NPAIR) {
-                                bw_do(inner);
-                                if (inner + 1 < NPAIR) bw_load(inner + 1);
-                            }
-                        } else if (inner == 0) {
-                            for (int p = 0; p < NPAIR; ++p) {
-                                bw_load(p);
-                                bw_do(p);
-                            }
+                        const int it = a.inner_it;
+                        for (int p = ((inner - stagger) % it + it) % it; p < NPAIR; p += it) {
+                            bw_load(p);
+                            bw_do(p);
                         }
                     }
                 }
@@ -457,11 +451,10 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
                 repeat = nx_repeat;
                 sh_j = nx_shj;
                 nrow = a.noise_f32 + (long long)nx_ts * a.inner_it * nstride + (long long)sh_j * M::NN;
-                if (ahead) bw_load(0);
             }
             if (pend && !aborted) {  // the last bw step
                 for (int p = 0; p < NPAIR; ++p) {
-                    if (p > 0 || !ahead) bw_load(p);
+                    bw_load(p);
                     bw_do(p);
                 }
             }
@@ -493,8 +486,10 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
+// 544 threads: the register file allows 96 registers a thread (warps are allocated
+// registers in groups of four, so 17 warps are charged as 20).
 template <class M>
-__global__ void __maxnreg__(120)
+__global__ void __launch_bounds__(PP_THREADS, 1)
     k_integrate_pp(const __grid_constant__ IntegrateArgs a, const int *work, int n_work, int KP, int use_sacc) {
     pp_body<M, false>(a, work, n_work, KP, use_sacc);
 }

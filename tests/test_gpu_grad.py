@@ -151,7 +151,7 @@ def test_tangent_dG_matches_fp64_finite_differences(model, G):
     differences of the FP64 path.  The tangent run's BOLD is the plain FP32 run's."""
     import torch
     from cubnm_b200 import core, grad, utils
-    N, nodes, dur = 3, 24, 5
+    N, nodes, dur = 3, 24, 8
     G = np.array(G)
     bold, dG = grad.bold_and_dG(_delayed_args(model, N, nodes, dur, 11, "fp32", G))
     plain = core.run_simulations(*_delayed_args(model, N, nodes, dur, 11, "fp32", G))["sim_bold"]

@@ -4,8 +4,9 @@ Balloon-Windkessel constants.
 * The README grid workload exactly (rWW, 4 x 5 x 5 = 100 simulations over G,
   w_p, J_N; 100 nodes; 60 s at dt 0.1 ms; TR 1 s; FC + FCD window 10 / step 2;
   SC at 30 % density), FIC off and analytical FIC on: FP64 GPU path against the
-  oracle on the same inputs and noise, |a - b| <= 1e-8 |b| + 1e-12 for BOLD,
-  FC, FCD and states, and every GOF term (through this library's GOF kernels)
+  oracle on the same inputs and noise, |a - b| <= 1e-8 |b| + 1e-12 for BOLD
+  and states and 1e-8 |b| + 1e-10 for FC and FCD (correlations: the absolute
+  term covers entries near zero), and every GOF term (through this library's GOF kernels)
   within 1e-8 of scipy's on the oracle's FC / FCD (the reference's CPU GOF,
   src/cubnm/sim/base.py:1176-1189).
 * The uneven-batch shapes with conduction delays (6 m/s over tract lengths of
@@ -31,6 +32,10 @@ from oracle import oracle
 pytestmark = pytest.mark.gpu
 
 RTOL, ATOL = 1e-8, 1e-12
+# FC and FCD are correlations (|r| <= 1): entries near zero get an absolute floor,
+# since there the relative difference is set by BOLD's last-ulp differences (CUDA's
+# and glibc's exp / pow); measured up to 7.4e-12 on 3 of 495,000 README-grid entries
+ATOL_R = 1e-10
 GOF_ATOL = 1e-8
 
 
@@ -41,7 +46,8 @@ def _copy(args):
 def _close(a, b, what):
     a, b = np.asarray(a), np.asarray(b)
     assert a.shape == b.shape, (what, a.shape, b.shape)
-    bad = np.abs(a - b) > RTOL * np.abs(b) + ATOL
+    atol = ATOL_R if what in ("sim_fc_trils", "sim_fcd_trils") else ATOL
+    bad = np.abs(a - b) > RTOL * np.abs(b) + atol
     assert not bad.any(), f"{what}: {bad.sum()} of {bad.size} outside 1e-8 relative; max abs {np.abs(a - b).max():.3e}"
 
 
