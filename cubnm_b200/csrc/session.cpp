@@ -328,7 +328,7 @@ struct Session {
     DBuf d_bold, d_states, d_gbools, d_gints, d_fc, d_fcd, d_wfc, d_pairs_i, d_pairs_j, d_wstart, d_wend, d_status;
     DBuf d_tiles, d_sct_f32, d_ell_pk, d_bw_scr, d_ln_groups, d_ln_params, d_ln_hist, d_ln_bw;
     DBuf fl_ec, fl_q, fl_win, fl_scr;  // fit loss
-    DBuf d_pidx;                       // tensor-core FC: pair index of (i, j)
+    DBuf d_pidx, d_wstat;              // tensor-core FC: pair index of (i, j); window-FC statistics
     // gof
     DBuf g_simfc, g_empfc, g_simfcd, g_empfcd, g_out;
     cbnm_timing timing{};
@@ -382,7 +382,7 @@ static void close_session(Session *&p) {
                         &S.d_g, &S.d_r, &S.d_v, &S.d_delay, &S.d_delay_idx, &S.d_max_delay, &S.d_hist_off,
                         &S.d_hist, &S.d_hist_f32, &S.d_bold, &S.d_states, &S.d_gbools, &S.d_gints, &S.d_fc,
                         &S.d_fcd, &S.d_wfc, &S.d_pairs_i, &S.d_pairs_j, &S.d_wstart, &S.d_wend, &S.d_status, &S.d_tiles,
-                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw, &S.fl_ec, &S.fl_q, &S.fl_win, &S.fl_scr, &S.d_pidx,
+                        &S.d_sct_f32, &S.d_ell_pk, &S.d_bw_scr, &S.d_ln_groups, &S.d_ln_params, &S.d_ln_hist, &S.d_ln_bw, &S.fl_ec, &S.fl_q, &S.fl_win, &S.fl_scr, &S.d_pidx, &S.d_wstat,
                         &S.g_simfc, &S.g_empfc, &S.g_simfcd, &S.g_empfcd, &S.g_out})
             b->release();
         for (auto &ev : S.ev) cudaEventDestroy(ev);
@@ -1302,6 +1302,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         const char *fce = std::getenv("CBNM_FC");
         const bool fc_tc = c.fp32 && (c.fc_tc || (fce && std::string(fce) == "tc"));
         if (fc_tc) {
+            if (c.do_fcd) fa.wstat = (double *)S.d_wstat.ensure(sizeof(double) * 2 * (size_t)chunk * std::max(1, c.n_windows));
             std::vector<int> pidx(nn, -1);
             for (size_t q = 0; q < pi.size(); ++q) pidx[(size_t)pi[q] * n + pj[q]] = (int)q;
             S.d_pidx.ensure(sizeof(int) * nn);
