@@ -38,7 +38,7 @@ class FitProblem:
     """One empirical target and the batched loss of candidate parameter sets."""
 
     def __init__(self, sc, emp_bold, duration_s, *, window_size=30, window_step=5, n_vols_remove=0, wIE=1.0,
-                 sigma=0.01, sim_seed=0, segment_steps=1000, device="cuda:0"):
+                 sigma=0.01, sim_seed=0, segment_steps=1000, device="cuda:0", fast_eval=False):
         import torch
         self.torch = torch
         self.nodes = sc.shape[0]
@@ -51,6 +51,7 @@ class FitProblem:
         self.wIE, self.sigma = wIE, sigma
         self.dim = 2 + self.nodes
         self.evals = 0
+        self.fast_eval = fast_eval
 
     def params_from_unit(self, x):
         """x [B, 2 + nodes] in [0, 1] -> G [B], w_p [B, nodes], J_N [B, nodes]."""
@@ -72,11 +73,32 @@ class FitProblem:
         return rww_fit_loss(bold, self.emp_fc, self.emp_fcd, self.remove, self.ws, self.step)
 
     def loss_np(self, x):
+        """Loss of candidates without gradients (grid, CMA-ES): with ``fast_eval`` on the
+        fastest FP32 forward kernel for the shape (cbnm_run_simulations_device) and the
+        loss kernels, else through the adjoint's forward pass."""
         torch = self.torch
         with torch.no_grad():
-            v = self.loss(torch.as_tensor(x, dtype=torch.float64, device=self.dev))
+            xt = torch.as_tensor(x, dtype=torch.float64, device=self.dev)
+            v = self._fast_loss(xt) if self.fast_eval else self.loss(xt)
         v = v.cpu().numpy()
         return np.where(np.isfinite(v), v, np.inf)
+
+    def _fast_loss(self, x):
+        from .grad import fit_loss_terms, run_device
+        G, w_p, J_N = self.params_from_unit(x)
+        B, n = x.shape[0], self.nodes
+        cfg = dict(self.prob.config)
+        cfg["precision"] = "fp32"
+        reg = np.stack([w_p.cpu().numpy().reshape(-1), J_N.cpu().numpy().reshape(-1), np.full(B * n, self.wIE),
+                        np.full(B * n, self.sigma)])
+        args = ["rWW", self.prob.sc.cpu().numpy(), np.zeros(B, np.int32), np.zeros(n * n),
+                G.cpu().numpy().reshape(1, B).astype(float), reg, np.zeros(B), cfg, False, False, False, False, False,
+                False, B, n, self.prob.duration_ms, self.prob.bold_tr, self.prob.bold_tr, self.prob.sim_seed,
+                self.prob.dt, self.prob.bw_dt]
+        bold = run_device(args, device=self.dev)
+        lf, ld, _ = fit_loss_terms(bold, self.emp_fc, self.emp_fcd, self.remove, self.ws, self.step)
+        self.evals += B
+        return lf + ld
 
 
 def adam_fit(fp, n_starts, iters, lr=0.6, seed=0):
@@ -197,10 +219,12 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--methods", default="grid,cmaes,adam", help="comma-separated subset of grid,cmaes,adam")
     ap.add_argument("--target", type=float, default=None, help="loss to time against (default: CMA-ES's best)")
+    ap.add_argument("--fast-eval", action="store_true",
+                    help="grid / CMA-ES evaluate on the fastest FP32 forward kernel instead of the adjoint's forward")
     o = ap.parse_args(argv)
     sc = synthetic_sc(o.nodes, 0.25, o.seed)
     emp = synthetic_emp_bold(o.nodes, o.duration, o.seed + 7)
-    fp = FitProblem(sc, emp, o.duration, window_size=o.window, window_step=o.step)
+    fp = FitProblem(sc, emp, o.duration, window_size=o.window, window_step=o.step, fast_eval=o.fast_eval)
     fp.loss_np(np.full((2, fp.dim), 0.5))  # warm-up: noise generation, allocations
     res = {}
     methods = o.methods.split(",")

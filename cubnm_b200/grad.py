@@ -311,19 +311,9 @@ _BOLD = _LazyBOLD
 _LOSS = _LazyLoss
 
 
-def bold_and_dG(args, device="cuda:0"):
-    """BOLD and dBOLD/dG of a batch given by the reference's 22 run_simulations
-    arguments (host arrays; precision "fp32", model rWW or WC, delays allowed):
-    both [N, bold_len, nodes] float64 torch tensors on ``device``.
-
-    The derivative comes from the tangent-linear integrator (forward mode along
-    each simulation's G, noise held fixed), so dL/dG of any loss on BOLD is
-    ``(dL/dBOLD * dBOLD/dG).sum((1, 2))``, e.g. with the loss kernels::
-
-        bold, dG = bold_and_dG(args)
-        lf, ld, db = fit_loss_terms(bold, emp_fc, emp_fcd, remove, ws, step, grad=True)
-        dL_dG = (db * dG).sum((1, 2))
-    """
+def _device_run(args, device, tangent):
+    """Runs the reference's 22 arguments (host arrays) with inputs and outputs in
+    device memory; returns (bold [N, bold_len, nodes], dBOLD/dG or None)."""
     import torch
     dev = torch.device(device)
     L = lib()
@@ -337,7 +327,7 @@ def bold_and_dG(args, device="cuda:0"):
     keep = {"sc": t(args[1]), "sc_idx": t(np.asarray(args[2], np.int32), torch.int32), "dist": t(args[3]),
             "g": t(args[4]), "r": t(args[5]), "v": t(args[6])}
     bold = torch.empty((N, sizes.bold_len, n), dtype=torch.float64, device=dev)
-    dG = torch.zeros_like(bold)
+    dG = torch.zeros_like(bold) if tangent else None
     fc = torch.empty((N, max(1, sizes.n_pairs)), dtype=torch.float64, device=dev)
     fcd = torch.empty((N, max(1, sizes.n_window_pairs)), dtype=torch.float64, device=dev)
     states = torch.empty((sizes.n_state_vars, N, n * (sizes.states_len if args[9] else 1)), dtype=torch.float64,
@@ -351,5 +341,31 @@ def bold_and_dG(args, device="cuda:0"):
     out = _abi.Outputs(dp(bold), dp(fc), dp(fcd), dp(states), C.cast(C.c_void_p(gb.data_ptr()), C.POINTER(C.c_uint8)),
                        C.cast(C.c_void_p(gi.data_ptr()), C.POINTER(C.c_int32)), None, None, None, 0.0, 0.0)
     torch.cuda.synchronize(dev)
-    check(L.cbnm_run_tangent_device(C.byref(a), C.byref(out), _ptr(dG)))
+    if tangent:
+        check(L.cbnm_run_tangent_device(C.byref(a), C.byref(out), _ptr(dG)))
+    else:
+        check(L.cbnm_run_simulations_device(C.byref(a), C.byref(out)))
     return bold, dG
+
+
+def run_device(args, device="cuda:0"):
+    """BOLD [N, bold_len, nodes] (float64 torch tensor on ``device``) of the batch
+    given by the reference's 22 run_simulations arguments, inputs and outputs in
+    device memory (cbnm_run_simulations_device)."""
+    return _device_run(args, device, tangent=False)[0]
+
+
+def bold_and_dG(args, device="cuda:0"):
+    """BOLD and dBOLD/dG of a batch given by the reference's 22 run_simulations
+    arguments (host arrays; precision "fp32", model rWW or WC, delays allowed):
+    both [N, bold_len, nodes] float64 torch tensors on ``device``.
+
+    The derivative comes from the tangent-linear integrator (forward mode along
+    each simulation's G, noise held fixed), so dL/dG of any loss on BOLD is
+    ``(dL/dBOLD * dBOLD/dG).sum((1, 2))``, e.g. with the loss kernels::
+
+        bold, dG = bold_and_dG(args)
+        lf, ld, db = fit_loss_terms(bold, emp_fc, emp_fcd, remove, ws, step, grad=True)
+        dL_dG = (db * dG).sum((1, 2))
+    """
+    return _device_run(args, device, tangent=True)
