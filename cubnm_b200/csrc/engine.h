@@ -8,6 +8,23 @@ namespace cbnm {
 
 enum ModelId { MODEL_RWW = 0, MODEL_WC = 1, MODEL_JR = 2, MODEL_KURAMOTO = 3, MODEL_RWWEX = 4 };
 
+// Raises `kernel`'s dynamic shared-memory limit to all the device allows (the
+// opt-in maximum less the kernel's static shared memory).  The limit belongs to
+// the function, process-wide, and the groups of a batch launch from several host
+// threads at once: a limit set to each launch's own size could be lowered by
+// another thread between its set and its launch.  Every caller sets this same
+// value, so none can.  The launch's own size is checked by its caller.
+template <class K>
+inline cudaError_t allow_dynamic_smem(K kernel) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 // Balloon-Windkessel constants (reference: src/ext/models/bw.cpp:4-22).
 struct BWConst {
     double dt, rho, alpha, tau, y, kappa, V_0, k1, k2, k3;

@@ -125,7 +125,7 @@ cudaError_t launch_fc(const FcArgs &a, cudaStream_t st, int *launches) {
     size_t smem = sizeof(double) * (size_t)(2 * a.nodes + maxT * a.nodes);
     int staged = 1;
     if (smem > 200 * 1024) { staged = 0; smem = sizeof(double) * 2 * a.nodes; }
-    cudaError_t e = cudaFuncSetAttribute(k_fc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_fc);
     if (e != cudaSuccess) return e;
     dim3 grid(a.sim_count, 1 + ((a.n_windows > 0) ? a.n_windows : 0));
     k_fc<<<grid, FC_THREADS, smem, st>>>(a, staged);

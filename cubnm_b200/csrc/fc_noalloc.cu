@@ -246,7 +246,7 @@ int fc_fcd_noalloc(const double *bold, int n_sims, int bold_len, int nodes, int 
     size_t smem = sizeof(double) * (size_t)(2 * nodes + (size_t)max_T * nodes);
     int staged = 1;
     if (smem > 200 * 1024) { staged = 0; smem = sizeof(double) * 2 * nodes; }
-    cudaError_t e = cudaFuncSetAttribute(k_fc_scratch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_fc_scratch);
     if (e != cudaSuccess) return fail_cuda(msg, cap, e);
     for (int s0 = 0; s0 < n_sims; s0 += chunk) {
         const int cnt = std::min(chunk, n_sims - s0);

@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fcd_tc(const FcArgs a, int NW
 cudaError_t launch_fc_tc(const FcArgs &a, const int *pidx, cudaStream_t st, int *launches) {
     const int nblk = (a.nodes + FT_N - 1) / FT_N;
     const size_t smem = (size_t)2 * FT_KC * FT_N * 2 + sizeof(FtSmem) + 64;
-    cudaError_t e = cudaFuncSetAttribute(k_fc_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_fc_tc);
     if (e != cudaSuccess) return e;
     dim3 grid(a.sim_count, 1 + a.n_windows, nblk * (nblk + 1) / 2);
     k_fc_tc<<<grid, FT_THREADS, smem, st>>>(a, pidx, nblk);
@@ -321,7 +321,7 @@ cudaError_t launch_fc_tc(const FcArgs &a, const int *pidx, cudaStream_t st, int 
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int NW = ((a.n_windows + 15) / 16) * 16;
     const size_t fsmem = (size_t)2 * FT_KC * NW * 2 + sizeof(FtSmem) + 64;
-    e = cudaFuncSetAttribute(k_fcd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+    e = allow_dynamic_smem(k_fcd_tc);
     if (e != cudaSuccess) return e;
     k_fcd_tc<<<a.sim_count, FT_THREADS, fsmem, st>>>(a, NW);
     if (launches) ++*launches;

@@ -4,7 +4,8 @@
 // src/ext/utils.cpp:21-52; pair order np.tril_indices(n, -1)); r = Pearson
 // correlation of the FC lower triangles; W1 = the 1-D Wasserstein distance of
 // the FCD value distributions by the midpoint rule on the simulated quantiles,
-// mean_i |sort(fcd)_i - q_i| with q_i = sorted_emp[floor((i + 1/2) m2 / m)].
+// mean_i |sort(fcd)_i - q_i| with q_i = sorted_emp[floor((i + 1/2) m2 / m)]
+// (the index in integer arithmetic, ((2i + 1) m2) / (2m)).
 //
 // Forward, per simulation s (one CTA per (s, window) for the FCs, one CTA per s
 // for the rest):
@@ -272,7 +273,7 @@ cudaError_t launch_fit_loss(const FitLossArgs &a, cudaStream_t st, int *launches
     int m2 = 1;
     while (m2 < std::max(1, a.n_window_pairs)) m2 <<= 1;
     const size_t smem = fit_loss_sort_smem(std::max(1, a.n_window_pairs));
-    e = cudaFuncSetAttribute(k_fl_loss, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_dynamic_smem(k_fl_loss);
     if (e != cudaSuccess) return e;
     k_fl_loss<<<a.sim_count, FL_THREADS, smem, st>>>(a, m2);
     e = cudaGetLastError();

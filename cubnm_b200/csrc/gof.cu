@@ -134,7 +134,7 @@ cudaError_t launch_gof(const GofArgs &a, cudaStream_t st, int *launches) {
         while (m1p < a.n_wp) m1p <<= 1;
         const size_t smem = sizeof(double) * (size_t)m1p;
         if (smem > gof_ks_smem_limit()) return cudaErrorInvalidValue;
-        e = cudaFuncSetAttribute(k_fcd_ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_dynamic_smem(k_fcd_ks);
         if (e != cudaSuccess) return e;
         k_fcd_ks<<<a.n_sims, GOF_THREADS, smem, st>>>(a, m1p);
         if (launches) ++*launches;

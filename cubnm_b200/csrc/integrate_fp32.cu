@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                 const int sim = sims[2 * pr + u];
                 if (tr && act && sim >= 0 && bi < a.bold_len)  // no slot for a sample past bold_len
                     a.bold[(size_t)sim * a.bold_len * n + (size_t)bi * n + j] =
-                        bw.V0k1 * (1 - q[u]) + bw.V0k2 * (1 - q[u] / nu[u]) + bw.V0k3 * (1 - nu[u]);
+                        bold64(q[u], nu[u], bw);
             }
             tmem_st16(col, w);
         };
@@ -424,7 +424,7 @@ cudaError_t launch_tc(const IntegrateArgs &a, const int *tiles, int n_tiles, cud
     // shared memory large enough that no more CTAs than TMEM holds land on one SM
     const size_t floor = T::CTAS_PER_SM == 2 ? 80 * 1024 : 120 * 1024;
     const size_t smem = std::max<size_t>(smem_bytes<T>(KP), floor);
-    cudaError_t e = cudaFuncSetAttribute(k_integrate_tc<M, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_integrate_tc<M, T>);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);

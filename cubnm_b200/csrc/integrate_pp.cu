@@ -342,7 +342,8 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
                 double x[2] = {bwx[0].x, bwx[0].y}, f[2] = {bwx[1].x, bwx[1].y};
                 double nu[2] = {bwx[2].x, bwx[2].y}, q[2] = {bwx[3].x, bwx[3].y};
                 const float z0 = zbuf[(2 * p) * NUPD + tid], z1 = zbuf[(2 * p + 1) * NUPD + tid];
-                bw_step64x2(x, f, nu, q, (double)z0, (double)z1, bw);
+                bw_step64_contracted(x[0], f[0], nu[0], q[0], (double)z0, bw);
+                bw_step64_contracted(x[1], f[1], nu[1], q[1], (double)z1, bw);
                 double2 *b = bw_ptr(p);
                 __stcg(b, make_double2(x[0], x[1]));
                 __stcg(b + n, make_double2(f[0], f[1]));
@@ -354,7 +355,7 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
                         const int sim = wd[1 + half_of(p) * PP_TN + g * PP_SPT + 2 * (p & 3) + u];
                         if (sim >= 0)
                             a.bold[(size_t)sim * a.bold_len * n + (size_t)pend_bi * n + j] =
-                                bw.V0k1 * (1 - q[u]) + bw.V0k2 * (1 - q[u] / nu[u]) + bw.V0k3 * (1 - nu[u]);
+                                bold64(q[u], nu[u], bw);
                     }
                 }
             };
@@ -515,11 +516,11 @@ cudaError_t launch_pp(const IntegrateArgs &a, cudaStream_t st) {
     const size_t smem = pp_smem<M>(KP, a.nodes, &use_sacc);
     const int grid = std::min(a.n_tiles, a.pp_grid);
     if (a.pp_ws) {
-        cudaError_t e = cudaFuncSetAttribute(k_integrate_pp_ws<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_dynamic_smem(k_integrate_pp_ws<M>);
         if (e != cudaSuccess) return e;
         k_integrate_pp_ws<M><<<grid, 1024, smem, st>>>(a, a.tiles, a.n_tiles, KP, use_sacc);
     } else {
-        cudaError_t e = cudaFuncSetAttribute(k_integrate_pp<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_dynamic_smem(k_integrate_pp<M>);
         if (e != cudaSuccess) return e;
         k_integrate_pp<M><<<grid, PP_THREADS, smem, st>>>(a, a.tiles, a.n_tiles, KP, use_sacc);
     }

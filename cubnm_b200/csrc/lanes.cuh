@@ -196,7 +196,7 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
             bj[2 * LN_SIMS] = nu;
             bj[3 * LN_SIMS] = q;
             if (tr && bold_i < a.bold_len)  // no slot for a sample past bold_len
-                bold[(size_t)bold_i * n + j] = bw.V0k1 * (1 - q) + bw.V0k2 * (1 - q / nu) + bw.V0k3 * (1 - nu);
+                bold[(size_t)bold_i * n + j] = bold64(q, nu, bw);
         }
         if (tr) bold_i++;
         if (sample) states_i++;

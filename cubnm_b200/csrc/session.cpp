@@ -1817,7 +1817,8 @@ static void fit_loss_impl(const double *bold, int n_sims, int bold_len, int node
         std::vector<double> es(emp_fcd, emp_fcd + n_emp_fcd);
         std::sort(es.begin(), es.end());
         for (int i = 0; i < M; ++i) {
-            const long long k = std::min<long long>(n_emp_fcd - 1, (long long)std::floor((i + 0.5) / M * n_emp_fcd));
+            // floor((i + 1/2) m2 / M) in integers (exact where the quotient is whole)
+            const long long k = std::min<long long>(n_emp_fcd - 1, (2LL * i + 1) * n_emp_fcd / (2LL * M));
             q[i] = es[k];
         }
     }

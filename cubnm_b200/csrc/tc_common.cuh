@@ -380,13 +380,28 @@ __device__ __forceinline__ double pow_omr(double f, double inv_f, const BW64 &c)
     return exp2(c.log2_omr / f);
 }
 
+// Every multiply-add below is spelled out (fma / __dmul_rn / __dadd_rn), so the
+// compiler's contraction choices, which can differ between the kernels this is
+// inlined into, never change a bit of the result: the same inputs give the same
+// BOLD in every integrator that uses it.
 __device__ __forceinline__ void bw_step64(double &x, double &f, double &nu, double &q, double z, const BW64 &c) {
-    x = x + c.dt * (z - c.kappa * x - c.y * (f - 1.0));
-    const double tmp_f = f + c.dt * x;
+    double t = fma(-c.kappa, x, z);
+    t = fma(-c.y, __dsub_rn(f, 1.0), t);
+    x = fma(c.dt, t, x);
+    const double tmp_f = fma(c.dt, x, f);
     const double inv_f = rcp_fast(f);
-    nu = nu + c.dt_itau * (f - pow_nu(nu, c));
-    q = q + c.dt_itau * (f * (1.0 - pow_omr(f, inv_f, c)) * c.irho - pow_nu(nu, c) * q * rcp_fast(nu));
+    nu = fma(c.dt_itau, __dsub_rn(f, pow_nu(nu, c)), nu);
+    const double in = __dmul_rn(__dmul_rn(f, __dsub_rn(1.0, pow_omr(f, inv_f, c))), c.irho);
+    const double out = __dmul_rn(__dmul_rn(pow_nu(nu, c), q), rcp_fast(nu));
+    q = fma(c.dt_itau, __dsub_rn(in, out), q);
     f = tmp_f;
+}
+
+// BOLD = V0 (k1 (1 - q) + k2 (1 - q / nu) + k3 (1 - nu))  (bnm.cpp:316-335)
+__device__ __forceinline__ double bold64(double q, double nu, const BW64 &c) {
+    double b = __dmul_rn(c.V0k1, __dsub_rn(1.0, q));
+    b = fma(c.V0k2, __dsub_rn(1.0, __ddiv_rn(q, nu)), b);
+    return fma(c.V0k3, __dsub_rn(1.0, nu), b);
 }
 
 __device__ __forceinline__ void bw_step64x2(double (&x)[2], double (&f)[2], double (&nu)[2], double (&q)[2],
@@ -394,6 +409,19 @@ __device__ __forceinline__ void bw_step64x2(double (&x)[2], double (&f)[2], doub
     const double z[2] = {z0, z1};
 #pragma unroll
     for (int u = 0; u < 2; ++u) bw_step64(x[u], f[u], nu[u], q[u], z[u], c);
+}
+
+// The same step with the multiply-adds left to the compiler.  The two-tile
+// kernel runs at its 96-register limit, where this form spills less; its
+// results may differ from bw_step64 in the last bits.
+__device__ __forceinline__ void bw_step64_contracted(double &x, double &f, double &nu, double &q, double z,
+                                                     const BW64 &c) {
+    x = x + c.dt * (z - c.kappa * x - c.y * (f - 1.0));
+    const double tmp_f = f + c.dt * x;
+    const double inv_f = rcp_fast(f);
+    nu = nu + c.dt_itau * (f - pow_nu(nu, c));
+    q = q + c.dt_itau * (f * (1.0 - pow_omr(f, inv_f, c)) * c.irho - pow_nu(nu, c) * q * rcp_fast(nu));
+    f = tmp_f;
 }
 
 }  // namespace

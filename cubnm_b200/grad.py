@@ -98,12 +98,14 @@ def fcd_wasserstein(sim_fcd, emp_fcd):
     distribution of each row of sim_fcd [N, m] and emp_fcd [m2], by the midpoint
     rule on the simulated quantiles: mean_i |sorted_sim[i] - Q_emp((i + 1/2)/m)|
     with Q_emp the empirical quantile function (sorted_emp[floor(p m2)]).  Exact
-    when m == m2; the gradient flows through the sorted simulated values."""
+    when m == m2; the gradient flows through the sorted simulated values.  The
+    index floor((i + 1/2) m2 / m) = ((2i + 1) m2) // (2m) is taken in integers:
+    in floating point it can fall one short where the quotient is a whole number."""
     import torch
     m, m2 = sim_fcd.shape[1], emp_fcd.numel()
     emp_sorted = torch.sort(emp_fcd.reshape(-1)).values
-    p = (torch.arange(m, dtype=sim_fcd.dtype, device=sim_fcd.device) + 0.5) / m
-    q = emp_sorted[torch.floor(p * m2).long().clamp(max=m2 - 1)]
+    i = torch.arange(m, dtype=torch.int64, device=sim_fcd.device)
+    q = emp_sorted[((2 * i + 1) * m2 // (2 * m)).clamp(max=m2 - 1)]
     return (torch.sort(sim_fcd, dim=1).values - q).abs().mean(dim=1)
 
 

@@ -73,3 +73,20 @@ def test_batch_reports_the_failing_group():
     bad[13] = True  # use_cpu
     with pytest.raises(RuntimeError, match="group 1: use_cpu"):
         core.run_batch([_copy(groups[0]), bad, _copy(groups[2])])
+
+
+def test_batch_groups_with_different_fc_shared_memory():
+    """Groups whose FC kernels stage windows of different sizes in shared memory
+    (40 and 300 nodes) launch from several host threads at once: a shared-memory
+    limit set per launch would let one group's setting fail another's launch."""
+    groups = []
+    for i in range(12):
+        nodes = 300 if i % 2 else 40
+        a = list(cases.synthetic_args("rWW", N=8, nodes=nodes, duration_s=40, seed=20 + i, density=0.2,
+                                      bold_remove_s=2, window_size=10, window_step=2, precision="fp32"))
+        groups.append(a)
+    bat = core.run_batch([_copy(g) for g in groups])
+    for i in (0, 1):
+        ref = core.run_simulations(*_copy(groups[i]))
+        np.testing.assert_array_equal(bat[i]["sim_fc_trils"], ref["sim_fc_trils"])
+        np.testing.assert_array_equal(bat[i]["sim_fcd_trils"], ref["sim_fcd_trils"])

@@ -144,11 +144,16 @@ def _delayed_args(model, N, nodes, duration_s, seed, precision, G):
     return args
 
 
-@pytest.mark.parametrize("model,G", [("WC", [0.4, 1.2, 2.5]), ("rWW", [0.5, 1.5, 3.0])])
+@pytest.mark.parametrize("model,G", [("WC", [0.4, 1.2, 1.8]), ("rWW", [0.5, 1.5, 3.0])])
 def test_tangent_dG_matches_fp64_finite_differences(model, G):
     """dL/dG of L = sum(w * BOLD) (fixed random weights) and of the fit loss, from
     dBOLD/dG of the tangent integrator (FP32 state, delays, 6 m/s), against central
-    differences of the FP64 path.  The tangent run's BOLD is the plain FP32 run's."""
+    differences of the FP64 path.  The tangent run's BOLD is the plain FP32 run's.
+
+    Every G here leaves the trajectory non-chaotic: on this network WC at G = 2.5
+    is chaotic (a 1e-9 relative change of G moves the FP64 BOLD by 5e-3 within
+    8 s), so its derivative grows exponentially and central differences cannot
+    check it."""
     import torch
     from cubnm_b200 import core, grad, utils
     N, nodes, dur = 3, 24, 8

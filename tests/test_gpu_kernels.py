@@ -105,8 +105,8 @@ def _delayed(model, nodes, N, duration_s, seed, density=0.2, v=6.0, window=(4, 2
                                                  ("WC", 300, 18, True), ("rWWEx", 68, 33, True),
                                                  ("rWW", 200, 24, False), ("JR", 160, 17, True)])
 def test_lane_kernel_matches_per_simulation_kernel(model, nodes, N, delay, monkeypatch):
-    args = _delayed(model, nodes, N, 6, seed=nodes) if delay else list(
-        cases.synthetic_args(model, N=N, nodes=nodes, duration_s=6, seed=nodes, density=0.25, window_size=4,
+    args = _delayed(model, nodes, N, 10, seed=nodes) if delay else list(
+        cases.synthetic_args(model, N=N, nodes=nodes, duration_s=10, seed=nodes, density=0.25, window_size=4,
                              window_step=2, bold_remove_s=2))
     lanes = core.run_simulations(*_with(args, precision="fp32"))
     monkeypatch.setenv("CBNM_FP32_KERNEL", "simt")
@@ -123,13 +123,13 @@ def test_lane_kernel_mixed_velocities_and_scs():
     """Groups are formed per (SC, delay table): two SCs x three velocities, with a
     count that leaves partly empty groups."""
     N, nodes = 45, 80
-    args = _delayed("rWW", nodes, N, 5, seed=8)
+    args = _delayed("rWW", nodes, N, 10, seed=8)
     args[1] = np.stack([cases.synthetic_sc(nodes, 0.2, s).reshape(-1) for s in (8, 9)])
     args[2] = (np.arange(N) % 2).astype(np.intc)
     args[6] = np.array([3.0, 6.0, 12.0])[np.arange(N) % 3]
     o64 = core.run_simulations(*_with(args, precision="fp64"))
     o32 = core.run_simulations(*_with(args, precision="fp32"))
-    _bounds(o64, o32, nodes, 5, 4, 2)
+    _bounds(o64, o32, nodes, 10, 4, 2)
 
 
 @pytest.mark.parametrize("nodes,N", [(100, 48), (400, 16)])
@@ -146,7 +146,7 @@ def test_lane_kernel_uneven_batch_shapes_within_bounds(nodes, N):
 def test_lane_kernel_large_sparse_wilson_cowan():
     """1,000 nodes at 10 % with delays (the large-network shape), FP32 vs FP64."""
     N, nodes = 4, 1000
-    args = _delayed("WC", nodes, N, 4, seed=4, density=0.1, window=(2, 1))
+    args = _delayed("WC", nodes, N, 8, seed=4, density=0.1, window=(2, 1))
     reg = args[5].reshape(8, N, nodes)
     reg[6] = reg[7] = 0.01
     o64 = core.run_simulations(*_with(args, precision="fp64"))
