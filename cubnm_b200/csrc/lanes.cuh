@@ -38,6 +38,7 @@ namespace cbnm {
 namespace lanes {
 
 constexpr int LN_SIMS = 16;   // simulations per group (a half-warp)
+constexpr int LN_GATHER_ROWS = 4;  // node rows of a thread whose coupling gathers are issued together
 
 template <bool TAN>
 __device__ __forceinline__ typename std::conditional<TAN, float2, float>::type hval(float x, float dx) {
@@ -71,6 +72,8 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
     constexpr int BWW = TAN ? 8 : 4;  // doubles of Balloon-Windkessel scratch per (node, simulation)
     using H = typename std::conditional<TAN, float2, float>::type;
     constexpr int ROW = NT / LN_SIMS;  // node rows per CTA
+    constexpr int LC = MN < LN_GATHER_ROWS ? MN : LN_GATHER_ROWS;   // rows whose gathers interleave
+    constexpr int QU = LC >= 4 ? 1 : 4 / LC;                          // nonzeros unrolled per row
     using R = float;
     const int tid = threadIdx.x;
     const int s = tid & (LN_SIMS - 1);
@@ -131,35 +134,50 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
         for (int inner = 0; inner < a.inner_it; ++inner) {
             const int hbase = buff * n;
             const bool out_now = sample && live && inner == a.inner_it - 1;
+            // rows in chunks of LC: the gathers of a chunk's rows interleave (q outer,
+            // row inner), so LC independent ring-buffer loads are in flight where one
+            // row alone would wait on each in turn; each row still sums its nonzeros
+            // in ascending order from zero
 #pragma unroll
-            for (int m = 0; m < MN; ++m) {
-                const int j = r0 + ROW * m;
-                if (j >= n) continue;
+            for (int m0 = 0; m0 < MN; m0 += LC) {
+                R in[LC], din[LC];
+#pragma unroll
+                for (int c = 0; c < LC; ++c) in[c] = din[c] = R(0);
                 // coupling: sum over the nonzeros of column j of SC[k][j] x_k(t - d_kj)
-                const int2 *pk = ell + j;
-                R in = R(0), din = R(0);
-#pragma unroll 4
+#pragma unroll QU
                 for (int q = 0; q < EK; ++q) {
-                    const int2 e = __ldg(pk + (size_t)q * n);
-                    int h = hbase + e.x + (delayed ? 0 : n);
-                    if (h >= hw) h -= hw;
-                    const H xk = hist[(size_t)h * LN_SIMS + s];
-                    if constexpr (TAN) {
-                        in += __int_as_float(e.y) * xk.x;
-                        din += __int_as_float(e.y) * xk.y;
-                    } else {
-                        in += __int_as_float(e.y) * xk;
+#pragma unroll
+                    for (int c = 0; c < LC; ++c) {
+                        const int j = r0 + ROW * (m0 + c);
+                        if (j >= n) continue;
+                        const int2 e = __ldg(ell + (size_t)q * n + j);
+                        int h = hbase + e.x + (delayed ? 0 : n);
+                        if (h >= hw) h -= hw;
+                        const H xk = hist[(size_t)h * LN_SIMS + s];
+                        if constexpr (TAN) {
+                            in[c] += __int_as_float(e.y) * xk.x;
+                            din[c] += __int_as_float(e.y) * xk.y;
+                        } else {
+                            in[c] += __int_as_float(e.y) * xk;
+                        }
                     }
                 }
-                const long long ni = ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
-                const R n0 = __ldg(a.noise_f32 + ni);
-                const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
-                R r[M::NR];
 #pragma unroll
-                for (int q = 0; q < M::NR; ++q) r[q] = __ldg(par + ((size_t)j * M::NR + q) * LN_SIMS + s);
-                if constexpr (TAN) TG::step(st[m], dst[m], iv, g, r, in, din, n0, n1, a.K);
-                else M::step(st[m], iv, g, r, in, n0, n1, a.K);
-                if (out_now) lanes_states_out<M::NS>(a, st[m], sim, j, states_i);
+                for (int c = 0; c < LC; ++c) {
+                    const int m = m0 + c;
+                    const int j = r0 + ROW * m;
+                    if (j >= n) continue;
+                    const long long ni =
+                        ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
+                    const R n0 = __ldg(a.noise_f32 + ni);
+                    const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
+                    R r[M::NR];
+#pragma unroll
+                    for (int q = 0; q < M::NR; ++q) r[q] = __ldg(par + ((size_t)j * M::NR + q) * LN_SIMS + s);
+                    if constexpr (TAN) TG::step(st[m], dst[m], iv, g, r, in[c], din[c], n0, n1, a.K);
+                    else M::step(st[m], iv, g, r, in[c], n0, n1, a.K);
+                    if (out_now) lanes_states_out<M::NS>(a, st[m], sim, j, states_i);
+                }
             }
 #pragma unroll
             for (int m = 0; m < MN; ++m) {
