@@ -28,6 +28,10 @@ constexpr int FT_N = 128;                       // nodes per block (MMA M and N)
 constexpr int FT_KC = 256;                      // volumes per chunk (multiple of 16)
 constexpr uint32_t FT_LBO = (FT_N / 8) * 128;   // K-direction core-matrix stride of B
 constexpr int FT_COL_A = FT_N;                  // TMEM: D [0, 128), A hi [128, 256), A lo [256, 384)
+// FCD: the accumulator restarts every FT_FLUSH chunks (1,024 node pairs, a chain of
+// at most 192 FP32 additions) and each group's sums are added into FP64 partials;
+// one accumulation over the 499,500 pairs of 1,000 nodes had drifted by ~1e-3.
+constexpr int FT_FLUSH = 4;
 
 struct FtSmem {
     uint64_t mbar;
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fc_tc(const FcArgs a, const i
                 const uint32_t tah = tmem + FT_COL_A + kk * 8, tal = tah + FT_KC / 2;
                 const uint64_t dbh = smem_desc(bh + kk * 2 * FT_LBO, FT_LBO, 128);
                 const uint64_t dbl = smem_desc(bl + kk * 2 * FT_LBO, FT_LBO, 128);
-                mma_bf16_ts(tmem, tah, dbh, idesc, (kc0 > 0 || kk > 0) ? 1u : 0u);
+                mma_bf16_ts(tmem, tah, dbh, idesc, (kc0 % (FT_FLUSH * FT_KC) > 0 || kk > 0) ? 1u : 0u);
                 mma_bf16_ts(tmem, tah, dbl, idesc, 1u);
                 mma_bf16_ts(tmem, tal, dbh, idesc, 1u);
             }
@@ -207,8 +211,10 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fcd_tc(const FcArgs a, int NW
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t lbo = (uint32_t)(NW / 8) * 128;   // K-direction core-matrix stride of B
     uint8_t *Bh = smem_raw, *Bl = smem_raw + (size_t)FT_KC * NW * 2;
-    FtSmem *sm = reinterpret_cast<FtSmem *>(smem_raw + (size_t)2 * FT_KC * NW * 2);
     const int ls = blockIdx.x, sim = a.sim_begin + ls, W = a.n_windows, P = a.n_pairs;
+    double *part = reinterpret_cast<double *>(smem_raw + (size_t)2 * FT_KC * NW * 2);  // FCD lower triangle
+    const int WP = W * (W - 1) / 2;
+    FtSmem *sm = reinterpret_cast<FtSmem *>(part + ((WP + 1) & ~1));
     const int tid = threadIdx.x, warp = tid >> 5;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm->tmem_base)),
@@ -219,6 +225,7 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fcd_tc(const FcArgs a, int NW
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm->mbar)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int k = tid; k < WP; k += blockDim.x) part[k] = 0.0;
     fence_before();
     __syncthreads();
     fence_after();
@@ -270,7 +277,7 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fcd_tc(const FcArgs a, int NW
                 const uint32_t tah = tmem + FT_COL_A + kk * 8, tal = tah + FT_KC / 2;
                 const uint64_t dbh = smem_desc(bh + kk * 2 * lbo, lbo, 128);
                 const uint64_t dbl = smem_desc(bl + kk * 2 * lbo, lbo, 128);
-                mma_bf16_ts(tmem, tah, dbh, idesc, (kc0 > 0 || kk > 0) ? 1u : 0u);
+                mma_bf16_ts(tmem, tah, dbh, idesc, (kc0 % (FT_FLUSH * FT_KC) > 0 || kk > 0) ? 1u : 0u);
                 mma_bf16_ts(tmem, tah, dbl, idesc, 1u);
                 mma_bf16_ts(tmem, tal, dbh, idesc, 1u);
             }
@@ -281,20 +288,23 @@ __global__ void __launch_bounds__(FT_THREADS, 1) k_fcd_tc(const FcArgs a, int NW
         fence_after();
         ok = __syncthreads_and(ok) != 0;
         if (!ok) break;
-    }
-    if (!ok) atomicExch(a.status_fc, 1);
-    double *out = a.fcd + (size_t)sim * a.n_window_pairs;
-    if (ok) {
-        for (int c0 = 0; c0 < NW; c0 += 16) {
-            uint32_t r[16];
-            tmem_ld16(t_lane + c0, r);
+        if ((kc0 / FT_KC) % FT_FLUSH == FT_FLUSH - 1 || kc0 + FT_KC >= K) {  // the group's sums into FP64
+            for (int c0 = 0; c0 < NW; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(t_lane + c0, r);
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                const int wb = c0 + c;
-                if (live && wb < tid) out[(size_t)tid * (tid - 1) / 2 + wb] = (double)__uint_as_float(r[c]);
+                for (int c = 0; c < 16; ++c) {
+                    const int wb = c0 + c;
+                    if (live && wb < tid) part[tid * (tid - 1) / 2 + wb] += (double)__uint_as_float(r[c]);
+                }
             }
         }
     }
+    if (!ok) atomicExch(a.status_fc, 1);
+    double *out = a.fcd + (size_t)sim * a.n_window_pairs;
+    __syncthreads();
+    if (ok)
+        for (int k = tid; k < WP; k += blockDim.x) out[k] = part[k];
     fence_before();
     __syncthreads();
     fence_after();
@@ -320,7 +330,8 @@ cudaError_t launch_fc_tc(const FcArgs &a, const int *pidx, cudaStream_t st, int 
     if (launches) ++*launches;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int NW = ((a.n_windows + 15) / 16) * 16;
-    const size_t fsmem = (size_t)2 * FT_KC * NW * 2 + sizeof(FtSmem) + 64;
+    const int WP = a.n_windows * (a.n_windows - 1) / 2;
+    const size_t fsmem = (size_t)2 * FT_KC * NW * 2 + sizeof(double) * ((WP + 1) & ~1) + sizeof(FtSmem) + 64;
     e = allow_dynamic_smem(k_fcd_tc);
     if (e != cudaSuccess) return e;
     k_fcd_tc<<<a.sim_count, FT_THREADS, fsmem, st>>>(a, NW);

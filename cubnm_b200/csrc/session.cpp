@@ -1037,6 +1037,22 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         f.omr = ia.bw.oneminrho;
         f.V0k1 = ia.bw.V_0 * ia.bw.k1; f.V0k2 = ia.bw.V_0 * ia.bw.k2; f.V0k3 = ia.bw.V_0 * ia.bw.k3;
         std::copy(ia.bw_binom, ia.bw_binom + 13, f.binom);
+        BW32 &g = ia.bw32;
+        const double rho = ia.bw.rho;
+        g.dt = (float)ia.bw.dt; g.kappa = (float)ia.bw.kappa; g.y = (float)ia.bw.y; g.dt_itau = (float)ia.bw.dt_itau;
+        g.c_omr = (float)((1.0 - rho) / rho); g.m_ln_omr = (float)(-std::log1p(-rho));
+        g.ialpha = (float)ia.bw.ialpha; g.log2_omr = (float)std::log2(1.0 - rho); g.irho = (float)(1.0 / rho);
+        g.V0k1 = (float)f.V0k1; g.V0k2 = (float)f.V0k2; g.V0k3 = (float)f.V0k3;
+        {
+            long double ca = 1.0L, cb = 1.0L;
+            const long double ea = (long double)ia.bw.ialpha, eb = ea - 1.0L;
+            for (int k = 1; k <= BW32_TERMS; ++k) {
+                ca = ca * (ea - (k - 1)) / k;
+                cb = cb * (eb - (k - 1)) / k;
+                g.a[k - 1] = (float)ca;
+                g.b[k - 1] = (float)cb;
+            }
+        }
         if (md.id == MODEL_RWW) {
             const RWW32::K k = RWW32::make(ia.K);
             static_assert(sizeof(k) <= sizeof(ia.k32), "FP32 constants");
