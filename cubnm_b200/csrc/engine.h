@@ -39,14 +39,15 @@ struct BWFast {
 };
 
 // Balloon-Windkessel constants of the FP32 deviation form (tc_common.cuh,
-// bw_step32): the state is x and the deviations F = f - 1, N = nu - 1, Q = q - 1.
+// bw_step32): the state is x and the deviations F = f - 1, N = nu - 1, Q = q - 1,
+// each as an FP32 (hi, lo) pair.
 constexpr int BW32_TERMS = 8;
 struct BW32 {
+    double V0k1, V0k2, V0k3;     // the BOLD readout is FP64
     float dt, kappa, y, dt_itau;
     float c_omr;                 // (1 - rho) / rho
     float m_ln_omr;              // -ln(1 - rho)
     float ialpha, log2_omr, irho;  // the general forms, outside the series' range
-    float V0k1, V0k2, V0k3;
     float a[BW32_TERMS];         // C(1/alpha, k), k = 1..8:      (1 + N)^(1/alpha) - 1     = sum a_k N^k
     float b[BW32_TERMS];         // C(1/alpha - 1, k), k = 1..8:  (1 + N)^(1/alpha - 1) - 1 = sum b_k N^k
 };

@@ -21,15 +21,15 @@
 //    slice to be read from shared memory per MMA.  Elementwise model updates run
 //    in FP32 registers.
 //  * The Balloon-Windkessel state (bnm.cu:357-371) lives in TMEM in the FP32
-//    deviation form of tc_common.cuh (x, f - 1, nu - 1, q - 1: 4 words per
-//    simulation; within 1.3e-8 of the FP64 step's BOLD).  The update of bw step m runs during the
+//    deviation form of tc_common.cuh (x, f - 1, nu - 1, q - 1 as hi / lo pairs:
+//    8 words per simulation).  The update of bw step m runs during the
 //    GEMMs of bw step m+1 (one simulation pair per inner step), from the inputs
 //    saved at the end of step m, so the FP64 work overlaps the tensor core.
 //  * Every wait on the MMA barrier is bounded; on timeout the CTA records a
 //    status, leaves its loop, frees its TMEM and returns.
 //
 // TMEM columns: [0, NACC TN) accumulator sets | [NACC TN, NACC TN + KP) SC^T hi then lo, two BF16
-// per column, K chunk kk at +8kk | [COLS - 4 TN, COLS) Balloon-Windkessel state.
+// per column, K chunk kk at +8kk | [COLS - 8 TN, COLS) Balloon-Windkessel state.
 // SMEM B operand (MN-major, no swizzle, 8-row x 16-byte core matrices):
 //   element (k, n) at (k/8)*LBO_B + (n/8)*128 + (k%8)*16 + (n%8)*2,
 //   LBO_B = TN/8 * 128 B (K-direction core-matrix stride), SBO = 128 B.
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
     constexpr int NACC = T::NACC;
     constexpr int SPT = T::SPT;
     constexpr int COL_A = TN * NACC;                   // A_hi at COL_A, A_lo at COL_A + KP/2 (bf16 pairs)
-    constexpr int COL_BWT = TMEM_COLS - TN * 4;        // Balloon-Windkessel state at the top
+    constexpr int COL_BWT = TMEM_COLS - TN * 8;        // Balloon-Windkessel state at the top
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *B_hi = smem_raw;
     uint8_t *B_lo = B_hi + KP * TN * 2;
@@ -153,9 +153,9 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                 if (sims[i] >= 0)
                     for (int v = 0; v < M::NOUT; ++v) a.states[((size_t)v * a.n_sims + sims[i]) * ext + j] = 0.0;
         }
-        {  // Balloon-Windkessel state in TMEM: x = 0, f - 1 = nu - 1 = q - 1 = 0
+        {  // Balloon-Windkessel state in TMEM: x = 0, f - 1 = nu - 1 = q - 1 = 0 (hi and lo)
             uint32_t w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-            for (int i = 0; i < SPT; i += 2) tmem_st8(t_lane + COL_BWT + (wg * SPT + i) * 4, w);
+            for (int i = 0; i < SPT; ++i) tmem_st8(t_lane + COL_BWT + (wg * SPT + i) * 8, w);
         }
         // A operand = SC^T in TMEM (row j = target node on lane j; K = source node,
         // two BF16 per 32-bit column), split hi / lo.  Rewritten only when the SC changes;
@@ -203,24 +203,26 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
         // Balloon-Windkessel of one bw step for simulation pair `pr`, inputs z0, z1
         // (the BOLD state at the end of that bw step), BOLD written when `tr`.
         auto bw_pair = [&](int pr, float z0, float z1, bool tr, int bi) {
-            uint32_t w[8];  // x, F, N, Q of simulation 2 pr, then of 2 pr + 1 (FP32 deviation form)
-            const uint32_t col = t_lane + COL_BWT + (wg * SPT + 2 * pr) * 4;
-            tmem_ld8(col, w);
-            float2 x = make_float2(__uint_as_float(w[0]), __uint_as_float(w[4]));
-            float2 F = make_float2(__uint_as_float(w[1]), __uint_as_float(w[5]));
-            float2 N = make_float2(__uint_as_float(w[2]), __uint_as_float(w[6]));
-            float2 Q = make_float2(__uint_as_float(w[3]), __uint_as_float(w[7]));
-            if (act) bw_step32x2(x, F, N, Q, make_float2(z0, z1), bw);
-            w[0] = __float_as_uint(x.x); w[1] = __float_as_uint(F.x); w[2] = __float_as_uint(N.x); w[3] = __float_as_uint(Q.x);
-            w[4] = __float_as_uint(x.y); w[5] = __float_as_uint(F.y); w[6] = __float_as_uint(N.y); w[7] = __float_as_uint(Q.y);
+            uint32_t w[16];  // x, F, N, Q, then their lo parts, of simulation 2 pr, then of 2 pr + 1
+            const uint32_t col = t_lane + COL_BWT + (wg * SPT + 2 * pr) * 8;
+            tmem_ld16(col, w);
+            float2 v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = make_float2(__uint_as_float(w[i]), __uint_as_float(w[8 + i]));
+            if (act) bw_step32x2(v, make_float2(z0, z1), bw);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                w[i] = __float_as_uint(v[i].x);
+                w[8 + i] = __float_as_uint(v[i].y);
+            }
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 const int sim = sims[2 * pr + u];
                 if (tr && act && sim >= 0 && bi < a.bold_len)  // no slot for a sample past bold_len
                     a.bold[(size_t)sim * a.bold_len * n + (size_t)bi * n + j] =
-                        (double)bold32(u ? N.y : N.x, u ? Q.y : Q.x, bw);
+                        u ? bold32(v[2].y, v[6].y, v[3].y, v[7].y, bw) : bold32(v[2].x, v[6].x, v[3].x, v[7].x, bw);
             }
-            tmem_st8(col, w);
+            tmem_st16(col, w);
         };
         // pending Balloon-Windkessel work of the previous bw step: its inputs and BOLD flag
         float zp[SPT];
@@ -424,9 +426,9 @@ cudaError_t launch_model(const IntegrateArgs &a, cudaStream_t st) {
     return cudaErrorInvalidValue;
 }
 
-// TMEM columns used: accumulator sets (NACC TN) + SC^T hi/lo (KP) + Balloon-Windkessel state (4 TN)
+// TMEM columns used: accumulator sets (NACC TN) + SC^T hi/lo (KP) + Balloon-Windkessel state (8 TN)
 template <class T>
-constexpr bool tmem_fits(int KP) { return T::NACC * T::TN + KP + 4 * T::TN <= T::TMEM_COLS; }
+constexpr bool tmem_fits(int KP) { return T::NACC * T::TN + KP + 8 * T::TN <= T::TMEM_COLS; }
 
 }  // namespace
 

@@ -39,6 +39,7 @@ namespace lanes {
 
 constexpr int LN_SIMS = 16;   // simulations per group (a half-warp)
 constexpr int LN_GATHER_ROWS = 4;  // node rows of a thread whose coupling gathers are issued together
+constexpr int LN_GATHER_MLP = 8;   // coupling gathers of a thread in flight (rows x nonzeros unrolled)
 
 template <bool TAN>
 __device__ __forceinline__ typename std::conditional<TAN, float2, float>::type hval(float x, float dx) {
@@ -73,7 +74,7 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
     using H = typename std::conditional<TAN, float2, float>::type;
     constexpr int ROW = NT / LN_SIMS;  // node rows per CTA
     constexpr int LC = MN < LN_GATHER_ROWS ? MN : LN_GATHER_ROWS;   // rows whose gathers interleave
-    constexpr int QU = LC >= 4 ? 1 : 4 / LC;                          // nonzeros unrolled per row
+    constexpr int QU = LC >= LN_GATHER_MLP ? 1 : LN_GATHER_MLP / LC;  // nonzeros unrolled per row
     using R = float;
     const int tid = threadIdx.x;
     const int s = tid & (LN_SIMS - 1);

@@ -399,10 +399,12 @@ __device__ __forceinline__ void bw_step64(double &x, double &f, double &nu, doub
 
 // ---- Balloon-Windkessel step in FP32, deviation form.
 // f, nu and q stay near 1, so the state is kept as x and the deviations
-// F = f - 1, N = nu - 1, Q = q - 1: FP32 then resolves them to ~1e-7 of their
-// own size (about 1e-9 absolute) where FP32 f, nu, q would carry 6e-8 absolute.
-// The step of bw_step64 rewritten in these variables (no approximation beyond
-// the truncated series below):
+// F = f - 1, N = nu - 1, Q = q - 1, and each of the four as an FP32 pair
+// (hi, lo): a step adds an increment of ~1e-7 to a value of ~0.1, and in one
+// FP32 word the rounding of those additions would random-walk over a run (60,000
+// steps) to the size of a quiet network's BOLD fluctuations.  The pair keeps the
+// sum to ~1e-15; the nonlinear terms are evaluated on hi.  The step of bw_step64
+// rewritten in these variables (no approximation beyond the truncated series):
 //   x' = x + dt (z - kappa x - y F)
 //   F' = F + dt x'
 //   N' = N + dt/tau (F - P_a(N)),             P_a(N) = (1 + N)^(1/alpha) - 1
@@ -410,15 +412,15 @@ __device__ __forceinline__ void bw_step64(double &x, double &f, double &nu, doub
 //     A - 1 = f (1 - (1 - rho)^(1/f)) / rho - 1 = F - c (1 + F) expm1(u),
 //             c = (1 - rho) / rho, u = -ln(1 - rho) F / (1 + F)
 //     B - 1 = nu'^(1/alpha - 1) q - 1 = P_b + Q + P_b Q,  P_b = (1 + N')^(1/alpha - 1) - 1
-//   BOLD = V0 (-k1 Q + k2 (N - Q) / (1 + N) - k3 N).
+//   BOLD = V0 (-k1 Q + k2 (N - Q) / (1 + N) - k3 N), in FP64 from hi + lo.
 // For |N| <= 1/4 the powers are their binomial series to N^8 (1/alpha = 3.125 is
 // near an integer, so the coefficients fall fast: first omitted term < 1e-8
 // relative), and for |F| <= 1/2 expm1 is its Taylor series to u^8 (|u| <= 0.42,
 // first omitted term < 1e-7 of the result at the edge, far less inside); outside
 // those ranges the general forms through exp2f / log2f are used.  (rWW's BOLD
 // input S_E <= 1 keeps F below ~0.45 and N below ~0.15.)  Against the FP64 step
-// over 60,000 steps of a rWW-like input, the FP32 deviation form's BOLD is within
-// 1.3e-8 (plain FP32 in f, nu, q: 1.9e-7).
+// over 30,000 steps of inputs fluctuating by 1e-2 to 1e-4, the BOLD stays within
+// 2e-5 of its own standard deviation (one FP32 word per variable: 6e-3).
 __device__ __forceinline__ float bw32_series(float N, const float *c) {  // sum_{k=1..8} c_{k-1} N^k
     float p = c[BW32_TERMS - 1];
 #pragma unroll
@@ -448,17 +450,31 @@ __device__ __forceinline__ float bw32_a1(float F, const BW32 &c) {  // A - 1
     const float E = exp2f(c.log2_omr / (1.0f + F));
     return (1.0f + F) * (1.0f - E) * c.irho - 1.0f;
 }
-__device__ __forceinline__ void bw_step32(float &x, float &F, float &N, float &Q, float z, const BW32 &c) {
-    x = fmaf(c.dt, fmaf(-c.y, F, fmaf(-c.kappa, x, z)), x);
-    const float Fn = fmaf(c.dt, x, F);
-    N = fmaf(c.dt_itau, F - bw32_pow1m(N, c.a, c.ialpha), N);
-    const float A1 = bw32_a1(F, c);
-    const float P = bw32_pow1m(N, c.b, c.ialpha - 1.0f);
-    Q = fmaf(c.dt_itau, A1 - fmaf(P, Q, P + Q), Q);
-    F = Fn;
+// (hi, lo) += d, renormalised (two Fast2Sum steps) so that lo stays below half an
+// ulp of hi; every operation rounds once (no contraction).
+__device__ __forceinline__ void bw32_acc(float &hi, float &lo, float d) {
+    const float s = __fadd_rn(hi, d);
+    lo = __fadd_rn(lo, __fsub_rn(d, __fsub_rn(s, hi)));
+    hi = __fadd_rn(s, lo);
+    lo = __fsub_rn(lo, __fsub_rn(hi, s));
 }
-// The same step for a simulation pair, two lanes per FFMA2; a pair outside the
-// series' range takes the scalar step.
+// v = {x, F, N, Q, x_lo, F_lo, N_lo, Q_lo}
+__device__ __forceinline__ void bw_step32(float (&v)[8], float z, const BW32 &c) {
+    const float dx = c.dt * fmaf(-c.y, v[1], fmaf(-c.kappa, v[0], z));
+    bw32_acc(v[0], v[4], dx);
+    const float dF = c.dt * v[0];
+    const float dN = c.dt_itau * (v[1] - bw32_pow1m(v[2], c.a, c.ialpha));
+    const float A1 = bw32_a1(v[1], c);
+    bw32_acc(v[2], v[6], dN);
+    const float P = bw32_pow1m(v[2], c.b, c.ialpha - 1.0f);
+    const float dQ = c.dt_itau * (A1 - fmaf(P, v[3], P + v[3]));
+    bw32_acc(v[3], v[7], dQ);
+    bw32_acc(v[1], v[5], dF);
+}
+
+// The same step for a simulation pair, two lanes per FFMA2 / FADD2; a pair
+// outside the series' range takes the scalar step.  v: the eight variables of
+// bw_step32, .x of the first simulation and .y of the second.
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }  // a - b, exact
 __device__ __forceinline__ float2 bw32_series2(float2 N, const float *c) {
     float2 p = f2(c[BW32_TERMS - 1]);
@@ -466,18 +482,30 @@ __device__ __forceinline__ float2 bw32_series2(float2 N, const float *c) {
     for (int k = BW32_TERMS - 2; k >= 0; --k) p = __ffma2_rn(p, N, f2(c[k]));
     return __fmul2_rn(p, N);
 }
-__device__ __forceinline__ void bw_step32x2(float2 &x, float2 &F, float2 &N, float2 &Q, float2 z, const BW32 &c) {
-    const bool in_range = fmaxf(fabsf(N.x), fabsf(N.y)) <= 0.2f && fmaxf(fabsf(F.x), fabsf(F.y)) <= 0.5f;
+__device__ __forceinline__ void bw32_acc2(float2 &hi, float2 &lo, float2 d) {
+    const float2 s = __fadd2_rn(hi, d);
+    lo = __fadd2_rn(lo, sub2(d, sub2(s, hi)));
+    hi = __fadd2_rn(s, lo);
+    lo = sub2(lo, sub2(hi, s));
+}
+__device__ __forceinline__ void bw_step32x2(float2 (&v)[8], float2 z, const BW32 &c) {
+    const bool in_range = fmaxf(fabsf(v[2].x), fabsf(v[2].y)) <= 0.2f && fmaxf(fabsf(v[1].x), fabsf(v[1].y)) <= 0.5f;
     if (!in_range) {  // N' stays within 1/4 when |N| <= 0.2, so the pair path needs no second check
-        bw_step32(x.x, F.x, N.x, Q.x, z.x, c);
-        bw_step32(x.y, F.y, N.y, Q.y, z.y, c);
+        float a[8], b[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) { a[i] = v[i].x; b[i] = v[i].y; }
+        bw_step32(a, z.x, c);
+        bw_step32(b, z.y, c);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = make_float2(a[i], b[i]);
         return;
     }
-    x = __ffma2_rn(f2(c.dt), __ffma2_rn(f2(-c.y), F, __ffma2_rn(f2(-c.kappa), x, z)), x);
-    const float2 Fn = __ffma2_rn(f2(c.dt), x, F);
-    N = __ffma2_rn(f2(c.dt_itau), sub2(F, bw32_series2(N, c.a)), N);
-    const float2 F1 = __fadd2_rn(F, f2(1.0f));
-    const float2 u = __fmul2_rn(__fmul2_rn(f2(c.m_ln_omr), F), make_float2(__frcp_rn(F1.x), __frcp_rn(F1.y)));
+    const float2 dx = __fmul2_rn(f2(c.dt), __ffma2_rn(f2(-c.y), v[1], __ffma2_rn(f2(-c.kappa), v[0], z)));
+    bw32_acc2(v[0], v[4], dx);
+    const float2 dF = __fmul2_rn(f2(c.dt), v[0]);
+    const float2 dN = __fmul2_rn(f2(c.dt_itau), sub2(v[1], bw32_series2(v[2], c.a)));
+    const float2 F1 = __fadd2_rn(v[1], f2(1.0f));
+    const float2 u = __fmul2_rn(__fmul2_rn(f2(c.m_ln_omr), v[1]), make_float2(__frcp_rn(F1.x), __frcp_rn(F1.y)));
     float2 e = f2(1.0f / 40320.0f);
     e = __ffma2_rn(e, u, f2(1.0f / 5040.0f));
     e = __ffma2_rn(e, u, f2(1.0f / 720.0f));
@@ -487,14 +515,18 @@ __device__ __forceinline__ void bw_step32x2(float2 &x, float2 &F, float2 &N, flo
     e = __ffma2_rn(e, u, f2(0.5f));
     e = __ffma2_rn(e, u, f2(1.0f));
     e = __fmul2_rn(e, u);
-    const float2 A1 = __ffma2_rn(__fmul2_rn(f2(-c.c_omr), e), F1, F);
-    const float2 P = bw32_series2(N, c.b);
-    Q = __ffma2_rn(f2(c.dt_itau), sub2(A1, __ffma2_rn(P, Q, __fadd2_rn(P, Q))), Q);
-    F = Fn;
+    const float2 A1 = __ffma2_rn(__fmul2_rn(f2(-c.c_omr), e), F1, v[1]);
+    bw32_acc2(v[2], v[6], dN);
+    const float2 P = bw32_series2(v[2], c.b);
+    const float2 dQ = __fmul2_rn(f2(c.dt_itau), sub2(A1, __ffma2_rn(P, v[3], __fadd2_rn(P, v[3]))));
+    bw32_acc2(v[3], v[7], dQ);
+    bw32_acc2(v[1], v[5], dF);
 }
 
-__device__ __forceinline__ float bold32(float N, float Q, const BW32 &c) {
-    return fmaf(-c.V0k1, Q, fmaf(c.V0k2, (N - Q) * __frcp_rn(1.0f + N), -c.V0k3 * N));
+// BOLD of the deviation state (hi, lo of N and Q), in FP64
+__device__ __forceinline__ double bold32(float N, float Nl, float Q, float Ql, const BW32 &c) {
+    const double n = (double)N + (double)Nl, q = (double)Q + (double)Ql;
+    return fma(-c.V0k1, q, fma(c.V0k2, (n - q) / (1.0 + n), -c.V0k3 * n));
 }
 
 // BOLD = V0 (k1 (1 - q) + k2 (1 - q / nu) + k3 (1 - nu))  (bnm.cpp:316-335)

@@ -32,7 +32,7 @@ def test_autotune_picks_an_applicable_integrator(delay, tmp_path, monkeypatch):
     a32[7] = dict(args[7], precision="fp32", autotune="1")
     o32 = core.run_simulations(*a32)
     first = core.last_integrator()
-    allowed = {"lanes", "lanes512", "simt"} if delay else {"tc2", "tc1", "lanes", "lanes512", "simt"}
+    allowed = {"lanes", "lanes512", "simt"} if delay else {"tc2", "tc2ws", "tc1", "lanes", "lanes512", "simt"}
     assert first in allowed
     lines = path.read_text().split("\n")
     assert len([l for l in lines if l.strip()]) == 1 and lines[0].split()[1] == first

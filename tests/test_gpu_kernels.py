@@ -1,7 +1,7 @@
 """The FP32 kernels against each other and against the FP64 path.
 
-* the two-tile tensor-core rWW kernel (default) against the single-tile one
-  (CBNM_FP32_TC=v5) and both against FP64: same bounds as the mixed-precision
+* the single-tile tensor-core rWW kernel (default) against the two-tile one
+  (CBNM_FP32_TC=pp, or ws for its warp-specialised form) and both against FP64: same bounds as the mixed-precision
   mode (|dFC| <= 2e-3, |dGOF| <= 1e-3), and the two tile forms close to each
   other (they differ only in the FP32 order in which the BF16x3 partial
   products are added);
@@ -57,14 +57,14 @@ def test_two_tile_kernel_matches_single_tile_and_fp64(N, monkeypatch):
     args = cases.synthetic_args("rWW", N=N, nodes=nodes, duration_s=16, seed=N, window_size=4, window_step=2,
                                 bold_remove_s=4)
     o64 = core.run_simulations(*_with(args, precision="fp64"))
+    v5 = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == "tc1"
+    monkeypatch.setenv("CBNM_FP32_TC", "pp")
     pp = core.run_simulations(*_with(args, precision="fp32"))
     assert core.last_integrator() == "tc2"
     monkeypatch.setenv("CBNM_FP32_TC", "ws")
     ws = core.run_simulations(*_with(args, precision="fp32"))
     assert core.last_integrator() == "tc2ws"
-    monkeypatch.setenv("CBNM_FP32_TC", "v5")
-    v5 = core.run_simulations(*_with(args, precision="fp32"))
-    assert core.last_integrator() == "tc1"
     monkeypatch.delenv("CBNM_FP32_TC")
     assert np.isfinite(pp["sim_bold"]).all()
     _bounds(o64, pp, nodes, 16, 4, 2)
@@ -76,9 +76,11 @@ def test_two_tile_kernel_matches_single_tile_and_fp64(N, monkeypatch):
     np.testing.assert_allclose(pp["_sim_states"], v5["_sim_states"], rtol=1e-3, atol=1e-4)
 
 
-def test_two_tile_kernel_mixed_scs_and_128_nodes():
-    """Simulations over three SCs interleaved (pairs within an SC only), 128 nodes
-    (every TMEM lane live; the state sums no longer fit in shared memory)."""
+@pytest.mark.parametrize("tc", ["v5", "pp"])
+def test_tile_kernels_mixed_scs_and_128_nodes(tc, monkeypatch):
+    """Simulations over three SCs interleaved (tiles / pairs within an SC only), 128
+    nodes (every TMEM lane live; the two-tile kernel's state sums no longer fit in
+    shared memory)."""
     N, nodes = 150, 128
     scs = np.stack([cases.synthetic_sc(nodes, 0.3, s).reshape(-1) for s in range(3)])
     args = list(cases.synthetic_args("rWW", N=N, nodes=nodes, duration_s=12, seed=5, window_size=4, window_step=2,
@@ -86,7 +88,9 @@ def test_two_tile_kernel_mixed_scs_and_128_nodes():
     args[1] = scs
     args[2] = (np.arange(N) % 3).astype(np.intc)
     o64 = core.run_simulations(*_with(args, precision="fp64"))
+    monkeypatch.setenv("CBNM_FP32_TC", tc)
     o32 = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == ("tc1" if tc == "v5" else "tc2")
     _bounds(o64, o32, nodes, 12, 4, 2)
     np.testing.assert_allclose(o32["_sim_states"], o64["_sim_states"], rtol=2e-3, atol=2e-3)
 
