@@ -83,6 +83,9 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
     uint8_t *B_hi = smem_raw;
     uint8_t *B_lo = B_hi + KP * TN * 2;
     Smem *sm = reinterpret_cast<Smem *>(B_lo + KP * TN * 2);
+    // time-averaged states: FP32 sums [NOUT][TN][n] in shared memory, written once per simulation
+    float *sacc = reinterpret_cast<float *>(B_lo + KP * TN * 2 + ((sizeof(Smem) + 15) & ~(size_t)15));
+    const bool use_sacc = a.ext_out && !a.states_ts;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -148,10 +151,9 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
             for (int q = 0; q < M::NS; ++q) s2[pr][q] = make_float2(sa[0][q], sa[1][q]);
             PairStep<M>::params(p2[pr]);
         }
-        if (a.ext_out && !a.states_ts && act) {  // states sums start at zero
+        if (use_sacc && act) {  // states sums start at zero
             for (int i = 0; i < SPT; ++i)
-                if (sims[i] >= 0)
-                    for (int v = 0; v < M::NOUT; ++v) a.states[((size_t)v * a.n_sims + sims[i]) * ext + j] = 0.0;
+                for (int v = 0; v < M::NOUT; ++v) sacc[((size_t)v * TN + wg * SPT + i) * n + j] = 0.0f;
         }
         {  // Balloon-Windkessel state in TMEM: x = 0, f - 1 = nu - 1 = q - 1 = 0 (hi and lo)
             uint32_t w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
@@ -345,13 +347,13 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
                                 const int sim = sims[2 * pr + u];
                                 if (sim < 0) continue;
                                 for (int v = 0; v < M::NOUT; ++v) {
-                                    const double ov = u ? o[v].y : o[v].x;
+                                    const float ov = u ? o[v].y : o[v].x;
                                     if (a.states_ts) {
                                         if (states_i < a.states_len)
                                             a.states[((size_t)v * a.n_sims + sim) * ext + (size_t)states_i * n + j] = ov;
                                     }
                                     else if (states_i >= a.n_states_samples_remove)
-                                        a.states[((size_t)v * a.n_sims + sim) * ext + j] += ov;
+                                        sacc[((size_t)v * TN + wg * SPT + 2 * pr + u) * n + j] += ov;
                                 }
                             }
                         }
@@ -381,11 +383,13 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
 #pragma unroll
             for (int pr = 0; pr < SPT / 2; ++pr) bw_pair(pr, zp[2 * pr], zp[2 * pr + 1], pend_tr, pend_bi);
         }
-        if (a.ext_out && !a.states_ts && act && !aborted) {
+        if (use_sacc && act && !aborted) {
             const int pts = states_i - a.n_states_samples_remove;
             for (int i = 0; i < SPT; ++i)
                 if (sims[i] >= 0)
-                    for (int v = 0; v < M::NOUT; ++v) a.states[((size_t)v * a.n_sims + sims[i]) * ext + j] /= pts;
+                    for (int v = 0; v < M::NOUT; ++v)
+                        a.states[((size_t)v * a.n_sims + sims[i]) * ext + j] =
+                            (double)sacc[((size_t)v * TN + wg * SPT + i) * n + j] / pts;
         }
         fence_before();
         __syncthreads();
@@ -402,13 +406,16 @@ using Tile32 = Tile<32, 8, 3>;   // 4 warpgroups x 8 simulations, one CTA per SM
 
 template <class T>
 size_t smem_bytes(int KP) { return (size_t)2 * KP * T::TN * 2 + sizeof(Smem) + 64; }
+// the time-averaged state sums [NOUT][TN][nodes] (FP32)
+template <class M, class T>
+size_t sacc_bytes(int nodes) { return sizeof(float) * (size_t)M::NOUT * T::TN * nodes + 16; }
 
 template <class M, class T>
 cudaError_t launch_tc(const IntegrateArgs &a, const int *tiles, int n_tiles, cudaStream_t st) {
     const int KP = ((a.nodes + 15) / 16) * 16;
     // shared memory large enough that no more CTAs than TMEM holds land on one SM
     const size_t floor = T::CTAS_PER_SM == 2 ? 80 * 1024 : 120 * 1024;
-    const size_t smem = std::max<size_t>(smem_bytes<T>(KP), floor);
+    const size_t smem = std::max<size_t>(smem_bytes<T>(KP) + sacc_bytes<M, T>(a.nodes), floor);
     cudaError_t e = allow_dynamic_smem(k_integrate_tc<M, T>);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
