@@ -26,6 +26,13 @@
 //    bw step, series form of tc_common.cuh); noise is shared by all simulations.
 // The coupling sum runs over the nonzeros in ascending source order from zero, as
 // the per-simulation kernel's, so the node states are the same as that kernel's.
+// A gather is two dependent loads (the entry, then x_k(t - d_kj), which for
+// networks whose ring buffers outgrow L2 comes from HBM), so the kernel is bound
+// by the loads in flight: a thread interleaves the gathers of LC of its rows
+// (nonzero q outer, row inner, unrolled to LN_GATHER_MLP gathers) and loads the
+// entries of nonzero q + 1 while those of q are in flight.  Registers are the
+// limit (64 a thread at 1,024 threads): the noise shuffle of a row is read per
+// step through L1 instead of being held per row.
 #pragma once
 #include <algorithm>
 #include <type_traits>
@@ -74,7 +81,10 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
     using H = typename std::conditional<TAN, float2, float>::type;
     constexpr int ROW = NT / LN_SIMS;  // node rows per CTA
     constexpr int LC = MN < LN_GATHER_ROWS ? MN : LN_GATHER_ROWS;   // rows whose gathers interleave
-    constexpr int QU = LC >= LN_GATHER_MLP ? 1 : LN_GATHER_MLP / LC;  // nonzeros unrolled per row
+    // gathers in flight: LN_GATHER_MLP with 8 or more rows a thread; 4 with fewer, where
+    // more (with the prefetched entries) spilled under the 64-register limit
+    constexpr int MLP = MN >= 8 ? LN_GATHER_MLP : 4;
+    constexpr int QU = LC >= MLP ? 1 : MLP / LC;                      // nonzeros unrolled per row
     using R = float;
     const int tid = threadIdx.x;
     const int s = tid & (LN_SIMS - 1);
@@ -125,9 +135,9 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
     __syncthreads();
 
     int buff = D, bold_i = 0, states_i = 0, repeat = 0;
-    int shj[MN];
-#pragma unroll
-    for (int m = 0; m < MN; ++m) shj[m] = (r0 + ROW * m < n) ? a.sh_nodes[r0 + ROW * m] : 0;
+    // the node shuffle of the current noise repeat (its row of a.sh_nodes), read per
+    // row and step through L1 rather than held in MN registers
+    const int *shn = a.sh_nodes;
     double *bold = a.bold + (size_t)(live ? sim : 0) * a.bold_len * n;
     for (int bw_i = 0; bw_i < a.bw_it; ++bw_i) {
         const int sh_ts = a.sh_ts[(bw_i % a.noise_bw_it) + repeat * a.noise_bw_it];
@@ -145,13 +155,28 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
 #pragma unroll
                 for (int c = 0; c < LC; ++c) in[c] = din[c] = R(0);
                 // coupling: sum over the nonzeros of column j of SC[k][j] x_k(t - d_kj)
+                // the ELLPACK entries of nonzero q + 1 load while the gathers of q are
+                // in flight (one iteration ahead), so the two dependent loads of a
+                // gather overlap across iterations
+                int2 ecur[LC];
+#pragma unroll
+                for (int c = 0; c < LC; ++c) {
+                    const int j = r0 + ROW * (m0 + c);
+                    ecur[c] = (j < n && EK > 0) ? __ldg(ell + j) : make_int2(0, 0);
+                }
 #pragma unroll QU
                 for (int q = 0; q < EK; ++q) {
+                    int2 enext[LC];
+#pragma unroll
+                    for (int c = 0; c < LC; ++c) {
+                        const int j = r0 + ROW * (m0 + c);
+                        enext[c] = (j < n && q + 1 < EK) ? __ldg(ell + (size_t)(q + 1) * n + j) : make_int2(0, 0);
+                    }
 #pragma unroll
                     for (int c = 0; c < LC; ++c) {
                         const int j = r0 + ROW * (m0 + c);
                         if (j >= n) continue;
-                        const int2 e = __ldg(ell + (size_t)q * n + j);
+                        const int2 e = ecur[c];
                         int h = hbase + e.x + (delayed ? 0 : n);
                         if (h >= hw) h -= hw;
                         const H xk = hist[(size_t)h * LN_SIMS + s];
@@ -162,6 +187,8 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
                             in[c] += __int_as_float(e.y) * xk;
                         }
                     }
+#pragma unroll
+                    for (int c = 0; c < LC; ++c) ecur[c] = enext[c];
                 }
 #pragma unroll
                 for (int c = 0; c < LC; ++c) {
@@ -169,7 +196,7 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
                     const int j = r0 + ROW * m;
                     if (j >= n) continue;
                     const long long ni =
-                        ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)shj[m] * M::NN;
+                        ((long long)sh_ts * a.inner_it + inner) * n * M::NN + (long long)__ldg(shn + j) * M::NN;
                     const R n0 = __ldg(a.noise_f32 + ni);
                     const R n1 = (M::NN > 1) ? __ldg(a.noise_f32 + ni + 1) : R(0);
                     R r[M::NR];
@@ -221,9 +248,7 @@ __device__ __forceinline__ void lanes_group(const IntegrateArgs &a, int gi,
         if (sample) states_i++;
         if ((bw_i + 1) % a.noise_bw_it == 0 && bw_i + 1 < a.bw_it) {
             repeat++;
-#pragma unroll
-            for (int m = 0; m < MN; ++m)
-                if (r0 + ROW * m < n) shj[m] = a.sh_nodes[(size_t)repeat * n + r0 + ROW * m];
+            shn = a.sh_nodes + (size_t)repeat * n;
         }
     }
     if (live && a.ext_out && !a.states_ts) {

@@ -915,11 +915,15 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         has_delay = *std::max_element(h_max_delay.begin(), h_max_delay.end()) > 0;
     }
     // FP32 kernels: the tensor-core tiles take shared-SC batches without delays or
-    // numerical FIC at <= 128 nodes; the lane kernel takes delays and larger
-    // networks of the models it implements; everything else in FP32 runs on the
-    // per-simulation kernel.  CBNM_FP32_KERNEL=simt forces the latter.
+    // numerical FIC at <= 128 nodes; everything else runs on the per-simulation
+    // kernel, which measured faster than the lane kernel on every delayed and
+    // large-network shape (1,000-node WC: 343 vs 218 sims x sim-s / s; 400-node
+    // rWW: 1,103 vs 435; 200-node rWW, 512 sims: 11,645 vs 1,593).  The lane kernel
+    // runs the G tangent, and when CBNM_FP32_KERNEL=lanes or the tuner picks it;
+    // CBNM_FP32_KERNEL=simt forces the per-simulation kernel everywhere.
     const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
     const bool force_simt = fp32_kernel && std::string(fp32_kernel) == "simt";
+    const bool force_lanes = fp32_kernel && std::string(fp32_kernel) == "lanes";
     const bool num_fic = c.do_fic && c.max_fic_trials > 0;
     if (tan_bold && (!c.fp32 || !lanes_tangent_supported(md.id) || num_fic || !lanes_supported(md.id, n, num_fic)))
         throw Err(CBNM_ERR_UNSUPPORTED, "the G tangent needs precision fp32, model rWW or WC, at most 1024 nodes and "
@@ -956,7 +960,7 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     }
     const bool use_tc = variant == V_DEFAULT ? (!tan_bold && !force_simt && tc_ok)
                                              : (variant == V_PP || variant == V_PPWS || variant == V_V5);
-    bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (!force_simt || tan_bold) && !use_tc)
+    bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (tan_bold || (force_lanes && !use_tc)))
                                           : (variant == V_LANES || variant == V_LANES512);
     const int lanes_threads = variant == V_LANES512 ? 512 : 1024;
     if (t_round && !t_round_resolved && !(use_lanes && lanes_threads == 1024 && !tan_bold && g_batch_launch)) {

@@ -476,11 +476,23 @@ __device__ __forceinline__ void bw_step32(float (&v)[8], float z, const BW32 &c)
 // outside the series' range takes the scalar step.  v: the eight variables of
 // bw_step32, .x of the first simulation and .y of the second.
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }  // a - b, exact
+// sum_{k=1..8} c_{k-1} N^k by Estrin's scheme (dependency depth 4 instead of
+// Horner's 8: the step runs while the update warps wait on the GEMM, where its
+// latency, not its instruction count, is what costs)
 __device__ __forceinline__ float2 bw32_series2(float2 N, const float *c) {
-    float2 p = f2(c[BW32_TERMS - 1]);
-#pragma unroll
-    for (int k = BW32_TERMS - 2; k >= 0; --k) p = __ffma2_rn(p, N, f2(c[k]));
-    return __fmul2_rn(p, N);
+    const float2 N2 = __fmul2_rn(N, N), N4 = __fmul2_rn(N2, N2);
+    const float2 q0 = __ffma2_rn(f2(c[1]), N, f2(c[0])), q1 = __ffma2_rn(f2(c[3]), N, f2(c[2]));
+    const float2 q2 = __ffma2_rn(f2(c[5]), N, f2(c[4])), q3 = __ffma2_rn(f2(c[7]), N, f2(c[6]));
+    const float2 r0 = __ffma2_rn(q1, N2, q0), r1 = __ffma2_rn(q3, N2, q2);
+    return __fmul2_rn(__ffma2_rn(r1, N4, r0), N);
+}
+__device__ __forceinline__ float2 bw32_expm12(float2 u) {  // sum_{k=1..8} u^k / k!, Estrin
+    const float2 u2 = __fmul2_rn(u, u), u4 = __fmul2_rn(u2, u2);
+    const float2 q0 = __ffma2_rn(f2(0.5f), u, f2(1.0f)), q1 = __ffma2_rn(f2(1.0f / 24.0f), u, f2(1.0f / 6.0f));
+    const float2 q2 = __ffma2_rn(f2(1.0f / 720.0f), u, f2(1.0f / 120.0f));
+    const float2 q3 = __ffma2_rn(f2(1.0f / 40320.0f), u, f2(1.0f / 5040.0f));
+    const float2 r0 = __ffma2_rn(q1, u2, q0), r1 = __ffma2_rn(q3, u2, q2);
+    return __fmul2_rn(__ffma2_rn(r1, u4, r0), u);
 }
 __device__ __forceinline__ void bw32_acc2(float2 &hi, float2 &lo, float2 d) {
     const float2 s = __fadd2_rn(hi, d);
@@ -488,6 +500,9 @@ __device__ __forceinline__ void bw32_acc2(float2 &hi, float2 &lo, float2 d) {
     hi = __fadd2_rn(s, lo);
     lo = sub2(lo, sub2(hi, s));
 }
+// The terms that depend on an updated variable (F' on x', Q' on N') read the plain
+// FP32 sum of the old value and its increment, so the four compensated additions,
+// independent of each other, come last and off the dependency chain.
 __device__ __forceinline__ void bw_step32x2(float2 (&v)[8], float2 z, const BW32 &c) {
     const bool in_range = fmaxf(fabsf(v[2].x), fabsf(v[2].y)) <= 0.2f && fmaxf(fabsf(v[1].x), fabsf(v[1].y)) <= 0.5f;
     if (!in_range) {  // N' stays within 1/4 when |N| <= 0.2, so the pair path needs no second check
@@ -501,26 +516,17 @@ __device__ __forceinline__ void bw_step32x2(float2 (&v)[8], float2 z, const BW32
         return;
     }
     const float2 dx = __fmul2_rn(f2(c.dt), __ffma2_rn(f2(-c.y), v[1], __ffma2_rn(f2(-c.kappa), v[0], z)));
-    bw32_acc2(v[0], v[4], dx);
-    const float2 dF = __fmul2_rn(f2(c.dt), v[0]);
+    const float2 dF = __fmul2_rn(f2(c.dt), __fadd2_rn(v[0], dx));
     const float2 dN = __fmul2_rn(f2(c.dt_itau), sub2(v[1], bw32_series2(v[2], c.a)));
     const float2 F1 = __fadd2_rn(v[1], f2(1.0f));
     const float2 u = __fmul2_rn(__fmul2_rn(f2(c.m_ln_omr), v[1]), make_float2(__frcp_rn(F1.x), __frcp_rn(F1.y)));
-    float2 e = f2(1.0f / 40320.0f);
-    e = __ffma2_rn(e, u, f2(1.0f / 5040.0f));
-    e = __ffma2_rn(e, u, f2(1.0f / 720.0f));
-    e = __ffma2_rn(e, u, f2(1.0f / 120.0f));
-    e = __ffma2_rn(e, u, f2(1.0f / 24.0f));
-    e = __ffma2_rn(e, u, f2(1.0f / 6.0f));
-    e = __ffma2_rn(e, u, f2(0.5f));
-    e = __ffma2_rn(e, u, f2(1.0f));
-    e = __fmul2_rn(e, u);
-    const float2 A1 = __ffma2_rn(__fmul2_rn(f2(-c.c_omr), e), F1, v[1]);
-    bw32_acc2(v[2], v[6], dN);
-    const float2 P = bw32_series2(v[2], c.b);
+    const float2 A1 = __ffma2_rn(__fmul2_rn(f2(-c.c_omr), bw32_expm12(u)), F1, v[1]);
+    const float2 P = bw32_series2(__fadd2_rn(v[2], dN), c.b);
     const float2 dQ = __fmul2_rn(f2(c.dt_itau), sub2(A1, __ffma2_rn(P, v[3], __fadd2_rn(P, v[3]))));
-    bw32_acc2(v[3], v[7], dQ);
+    bw32_acc2(v[0], v[4], dx);
     bw32_acc2(v[1], v[5], dF);
+    bw32_acc2(v[2], v[6], dN);
+    bw32_acc2(v[3], v[7], dQ);
 }
 
 // BOLD of the deviation state (hi, lo of N and Q), in FP64

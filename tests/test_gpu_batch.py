@@ -1,6 +1,7 @@
 """cbnm_run_batch (core.run_batch): independent groups run concurrently, each on
-its own stream; every group's outputs must equal a separate run_simulations call
-of the same arguments, bit for bit."""
+its own stream (or, for groups on the lane kernel, in one persistent launch per
+round); every group's outputs must equal a separate run_simulations call of the
+same arguments, bit for bit."""
 import numpy as np
 import pytest
 
@@ -40,7 +41,13 @@ def _copy(a):
     return [x.copy() if isinstance(x, np.ndarray) else x for x in a]
 
 
-def test_batch_equals_separate_calls():
+@pytest.mark.parametrize("kernel", ["default", "lanes"])
+def test_batch_equals_separate_calls(kernel, monkeypatch):
+    """With the lane kernel forced, the delayed and large groups of a round run as
+    one persistent work-queue launch (k_integrate_lanes_multi) and must still equal
+    their separate calls, which run k_integrate_lanes, bit for bit."""
+    if kernel == "lanes":
+        monkeypatch.setenv("CBNM_FP32_KERNEL", "lanes")
     groups = _groups()
     sep_args = [_copy(g) for g in groups]
     sep = [core.run_simulations(*a) for a in sep_args]

@@ -112,7 +112,9 @@ def test_lane_kernel_matches_per_simulation_kernel(model, nodes, N, delay, monke
     args = _delayed(model, nodes, N, 10, seed=nodes) if delay else list(
         cases.synthetic_args(model, N=N, nodes=nodes, duration_s=10, seed=nodes, density=0.25, window_size=4,
                              window_step=2, bold_remove_s=2))
+    monkeypatch.setenv("CBNM_FP32_KERNEL", "lanes")
     lanes = core.run_simulations(*_with(args, precision="fp32"))
+    assert core.last_integrator() == "lanes"
     monkeypatch.setenv("CBNM_FP32_KERNEL", "simt")
     monkeypatch.setenv("CBNM_COUPLING", "sparse")
     simt = core.run_simulations(*_with(args, precision="fp32"))
@@ -123,9 +125,10 @@ def test_lane_kernel_matches_per_simulation_kernel(model, nodes, N, delay, monke
     np.testing.assert_allclose(lanes["sim_fc_trils"], simt["sim_fc_trils"], rtol=0, atol=1e-4)
 
 
-def test_lane_kernel_mixed_velocities_and_scs():
+def test_lane_kernel_mixed_velocities_and_scs(monkeypatch):
     """Groups are formed per (SC, delay table): two SCs x three velocities, with a
     count that leaves partly empty groups."""
+    monkeypatch.setenv("CBNM_FP32_KERNEL", "lanes")
     N, nodes = 45, 80
     args = _delayed("rWW", nodes, N, 10, seed=8)
     args[1] = np.stack([cases.synthetic_sc(nodes, 0.2, s).reshape(-1) for s in (8, 9)])
@@ -137,9 +140,10 @@ def test_lane_kernel_mixed_velocities_and_scs():
 
 
 @pytest.mark.parametrize("nodes,N", [(100, 48), (400, 16)])
-def test_lane_kernel_uneven_batch_shapes_within_bounds(nodes, N):
+def test_lane_kernel_uneven_batch_shapes_within_bounds(nodes, N, monkeypatch):
     """The uneven-batch shapes (delays up to ~30 ms at 6 m/s, SC 20 %) in FP32
     against FP64 on the same noise."""
+    monkeypatch.setenv("CBNM_FP32_KERNEL", "lanes")
     args = _delayed("rWW", nodes, N, 20 if nodes == 100 else 8, seed=nodes,
                     window=(4, 2) if nodes == 100 else (2, 1))
     o64 = core.run_simulations(*_with(args, precision="fp64"))
@@ -147,8 +151,11 @@ def test_lane_kernel_uneven_batch_shapes_within_bounds(nodes, N):
     _bounds(o64, o32, nodes, 20 if nodes == 100 else 8, *((4, 2) if nodes == 100 else (2, 1)))
 
 
-def test_lane_kernel_large_sparse_wilson_cowan():
-    """1,000 nodes at 10 % with delays (the large-network shape), FP32 vs FP64."""
+@pytest.mark.parametrize("kernel", ["lanes", "simt"])
+def test_large_sparse_wilson_cowan(kernel, monkeypatch):
+    """1,000 nodes at 10 % with delays (the large-network shape), FP32 vs FP64, on
+    the lane kernel and the per-simulation kernel (the default)."""
+    monkeypatch.setenv("CBNM_FP32_KERNEL", kernel)
     N, nodes = 4, 1000
     args = _delayed("WC", nodes, N, 8, seed=4, density=0.1, window=(2, 1))
     reg = args[5].reshape(8, N, nodes)
