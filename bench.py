@@ -51,6 +51,11 @@ TRAFFIC_SOURCE = None
 # state additions 2
 RWW_FP32_FLOPS = 38
 WORKLOAD = f"rWW {NODES} nodes, {N_SIMS} sims, {DURATION_S} s, dt 0.1 ms, TR 1 s, FC+FCD w10/s2"
+# the kernel behind each integrator name of core.last_integrator()
+KERNEL_OF = {"tc1": "k_integrate_tc<RWW32, Tile<32, 8, 3>>", "tc2": "k_integrate_pp<RWW32>",
+             "tc2ws": "k_integrate_pp_ws<RWW32>", "simt": "k_integrate_sim<M, delay, float>",
+             "lanes": "k_integrate_lanes<M, 1024, ...>", "lanes512": "k_integrate_lanes<M, 512, ...>",
+             "fp64": "k_integrate_sim<M, delay, double>"}
 METRIC = "rWW sims x sim-s per wall-s (100 nodes, 32k sims)"
 UNIT = "sims*sim-s/s"
 
@@ -286,7 +291,7 @@ def run_ours(opts, rank, world, local_rank):
                        "mma_issued_tflops": issued / integ / 1e12},
             "traffic": traffic, "traffic_source": traffic_src,
             "algorithmic_bytes": N_SIMS * NODES * DURATION_S * 8.0 if n_sims == N_SIMS else None,
-            "kernel": "k_integrate_pp<RWW32>", "kernel_ms": integ * 1e3,
+            "kernel": KERNEL_OF.get(core.last_integrator(), core.last_integrator()), "kernel_ms": integ * 1e3,
             "note": "per-pipe utilisation of this kernel: profiles/ (ncu)"}
 
     line = {
@@ -463,6 +468,35 @@ def _oracle_sample(args, sample, duration_s=None):
     return sample * a[16] / 1000 / el, el
 
 
+def config_roofline(args, integrate_ms, delayed, fp32_peak=None):
+    """Roofline of the integrator of a c2-c4 workload (per launch, mean CUDA-event
+    time of the integrator).  Delayed networks: the ring-buffer gathers, 4 bytes per
+    nonzero of the target's SC column per node-step, against the measured HBM copy
+    bandwidth (no credit taken for L2 hits).  Without delays (c3): the FP32 work of a
+    node-step (2 flops per nonzero of the coupling + the rWW update) against the
+    measured FP32 peak."""
+    from cubnm_b200 import core
+    N, n = args[14], args[15]
+    sc = np.asarray(args[1]).reshape(-1, n, n)
+    nnz = float(np.count_nonzero(sc[np.asarray(args[2], dtype=int)])) / (N * n)  # mean nonzeros per target
+    node_steps = N * n * (args[16] / args[20])
+    t = integrate_ms / 1e3
+    kernel = KERNEL_OF.get(core.last_integrator(), core.last_integrator())
+    if delayed:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        b = node_steps * nnz * 4.0
+        return {"bound": "hbm", "achieved": b / t / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": b / t / 1e9 / peaks["hbm_gbs"], "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "traffic": None, "algorithmic_bytes": b,
+                "work": f"{nnz:.1f} ring-buffer gathers x 4 B per node-step, {node_steps:.3e} node-steps",
+                "kernel": kernel, "kernel_ms": integrate_ms}
+    flops = node_steps * (2.0 * nnz + RWW_FP32_FLOPS)
+    return {"bound": "fp32", "achieved": flops / t / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": flops / t / 1e12 / fp32_peak, "peak_source": "measured on this GPU by cbnm_measure_fp32_peak",
+            "traffic": None, "work": f"2 x {nnz:.1f} coupling + {RWW_FP32_FLOPS} update FP32 flops per node-step, "
+                                     f"{node_steps:.3e} node-steps", "kernel": kernel, "kernel_ms": integrate_ms}
+
+
 def run_config(opts):
     import torch
     from cubnm_b200 import _abi, core, synthetic, utils
@@ -576,8 +610,11 @@ def run_config(opts):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         launches = 0
+        integ = []
         for _ in range(opts.steps):
-            launches += step()["kernel_launches"]
+            t = step()
+            launches += t["kernel_launches"]
+            integ.append(t["integrate_ms"])
         e1.record(st)
         torch.cuda.synchronize()
         ck = clocks.stop()
@@ -613,7 +650,10 @@ def run_config(opts):
         v, el = _oracle_sample(args, 2 * threads, duration_s=10)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{2 * threads} sims x 10 s of the workload, {el:.1f} s wall"}
-        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+        f1, f2 = C.c_double(), C.c_double()
+        check(L.cbnm_measure_fp32_peak(C.byref(f1), C.byref(f2)))
+        dtype = "f32 (FP64 Balloon-Windkessel)"
+        roof = config_roofline(args, float(np.mean(integ)), False, max(f1.value, f2.value))
     else:  # c4
         scale = opts.scale or 30.0
         dur = max(2, int(round(300 / scale)))
@@ -630,8 +670,11 @@ def run_config(opts):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         launches = 0
+        integ = []
         for _ in range(opts.steps):
-            launches += step()["kernel_launches"]
+            t = step()
+            launches += t["kernel_launches"]
+            integ.append(t["integrate_ms"])
         e1.record(st)
         torch.cuda.synchronize()
         ck = clocks.stop()
@@ -646,7 +689,8 @@ def run_config(opts):
         v, el = _oracle_sample(args, threads, duration_s=1)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{threads} sims x 1 s of the workload, {el:.1f} s wall"}
-        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+        dtype = "f32 (FP64 Balloon-Windkessel)"
+        roof = config_roofline(args, float(np.mean(integ)), True)
         extra["scale"] = scale
     line = {"metric": f"sims x sim-s per wall-s ({opts.config})", "value": value, "unit": UNIT, "n_gpus": 1,
             "steps": opts.steps, "warmup": opts.warmup, "ms_per_step": ms, "higher_is_better": True,

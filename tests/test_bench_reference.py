@@ -37,3 +37,24 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_config_roofline_counts_gathers_and_flops():
+    """The c2-c4 roofline: ring-buffer bytes (4 per nonzero per node-step) for delayed
+    networks, FP32 flops (2 per nonzero + the rWW update) without delays, per launch."""
+    import numpy as np
+    import bench
+    from cubnm_b200 import synthetic
+    args = list(synthetic.synthetic_args("rWW", N=4, nodes=20, duration_s=2, seed=1, density=0.25))
+    n = 20
+    sc = np.asarray(args[1]).reshape(n, n)
+    nnz = np.count_nonzero(sc) / n
+    node_steps = 4 * n * 2000 / 0.1
+    r = bench.config_roofline(args, 1000.0, True)
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert abs(r["algorithmic_bytes"] - node_steps * nnz * 4) < 1e-6 * r["algorithmic_bytes"]
+    assert abs(r["achieved"] - node_steps * nnz * 4 / 1e9) < 1e-9 * r["achieved"]
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    f = bench.config_roofline(args, 500.0, False, fp32_peak=70.0)
+    flops = node_steps * (2 * nnz + bench.RWW_FP32_FLOPS)
+    assert f["bound"] == "fp32" and abs(f["achieved"] - flops / 0.5 / 1e12) < 1e-9 * f["achieved"]
