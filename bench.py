@@ -297,7 +297,7 @@ def run_ours(opts, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": opts.steps,
         "warmup": opts.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (BF16x3 tensor-core coupling, FP32 deviation-form Balloon-Windkessel, FP64 FC/FCD)",
+        "vs_baseline": None, "dtype": "f32 (BF16x3 tensor-core coupling, FP64 Balloon-Windkessel and FC/FCD)",
         "data": "synthetic (seeded SC, parameters and noise)",
         "config": {"workload": WORKLOAD, "sims_per_gpu": n_sims, "nodes": NODES, "duration_s": opts.duration,
                    "precision": opts.precision, "parallelism": f"independent sims x{world}",

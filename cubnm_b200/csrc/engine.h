@@ -38,20 +38,6 @@ struct BWFast {
     double binom[13];            // C(1/alpha, k), k = 0..12
 };
 
-// Balloon-Windkessel constants of the FP32 deviation form (tc_common.cuh,
-// bw_step32): the state is x and the deviations F = f - 1, N = nu - 1, Q = q - 1,
-// each as an FP32 (hi, lo) pair.
-constexpr int BW32_TERMS = 8;
-struct BW32 {
-    double V0k1, V0k2, V0k3;     // the BOLD readout is FP64
-    float dt, kappa, y, dt_itau;
-    float c_omr;                 // (1 - rho) / rho
-    float m_ln_omr;              // -ln(1 - rho)
-    float ialpha, log2_omr, irho;  // the general forms, outside the series' range
-    float a[BW32_TERMS];         // C(1/alpha, k), k = 1..8:      (1 + N)^(1/alpha) - 1     = sum a_k N^k
-    float b[BW32_TERMS];         // C(1/alpha - 1, k), k = 1..8:  (1 + N)^(1/alpha - 1) - 1 = sum b_k N^k
-};
-
 // Model constants, computed on the host exactly as the reference's
 // init_constants(dt) does (src/ext/models/<model>.cpp).
 struct RWWK {
@@ -116,7 +102,6 @@ struct IntegrateArgs {
     int tile_width;              // FP32 kernel: simulations per tile (16 or 32)
     double bw_binom[13];         // FP32 kernel: binomial coefficients C(1/alpha, k), k = 0..12
     BWFast bwf;                  // two-tile kernel: Balloon-Windkessel constants
-    BW32 bw32;                   // FP32 deviation form of the Balloon-Windkessel step (bw_step32)
     alignas(8) float k32[24];    // two-tile kernel: the model's FP32 constants (M::K)
     int *status;                 // device status word (0 = ok)
     double *bw_scratch;          // two-tile kernel: per-CTA Balloon-Windkessel state (pp_bw_scratch_bytes)

@@ -20,9 +20,8 @@
 //    the tensor pipe then bounds the GEMM).  Keeping A in TMEM leaves only the 16-column x
 //    slice to be read from shared memory per MMA.  Elementwise model updates run
 //    in FP32 registers.
-//  * The Balloon-Windkessel state (bnm.cu:357-371) lives in TMEM in the FP32
-//    deviation form of tc_common.cuh (x, f - 1, nu - 1, q - 1 as hi / lo pairs:
-//    8 words per simulation).  The update of bw step m runs during the
+//  * The Balloon-Windkessel state (bnm.cu:357-371) stays FP64 and lives in TMEM
+//    (8 x 32-bit words per simulation).  The update of bw step m runs during the
 //    GEMMs of bw step m+1 (one simulation pair per inner step), from the inputs
 //    saved at the end of step m, so the FP64 work overlaps the tensor core.
 //  * Every wait on the MMA barrier is bounded; on timeout the CTA records a
@@ -116,7 +115,7 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
     uint32_t phase = 0;
     const uint32_t idesc = instr_desc(TN);
     const typename M::K K = M::make(a.K);
-    const BW32 &bw = a.bw32;
+    const BW64 &bw = a.bwf;
     const size_t rstride = (size_t)a.n_sims * n;
     const size_t ext = a.states_ts ? (size_t)n * a.states_len : (size_t)n;
     const int half = KP / 2;
@@ -155,8 +154,13 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
             for (int i = 0; i < SPT; ++i)
                 for (int v = 0; v < M::NOUT; ++v) sacc[((size_t)v * TN + wg * SPT + i) * n + j] = 0.0f;
         }
-        {  // Balloon-Windkessel state in TMEM: x = 0, f - 1 = nu - 1 = q - 1 = 0 (hi and lo)
-            uint32_t w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        {  // Balloon-Windkessel state in TMEM: x = 0, f = nu = q = 1
+            uint32_t w[8];
+            const double init[4] = {0.0, 1.0, 1.0, 1.0};
+            for (int q = 0; q < 4; ++q) {
+                w[2 * q] = (uint32_t)__double2loint(init[q]);
+                w[2 * q + 1] = (uint32_t)__double2hiint(init[q]);
+            }
             for (int i = 0; i < SPT; ++i) tmem_st8(t_lane + COL_BWT + (wg * SPT + i) * 8, w);
         }
         // A operand = SC^T in TMEM (row j = target node on lane j; K = source node,
@@ -205,24 +209,27 @@ __global__ void __launch_bounds__(T::NTHREADS, T::CTAS_PER_SM) k_integrate_tc(co
         // Balloon-Windkessel of one bw step for simulation pair `pr`, inputs z0, z1
         // (the BOLD state at the end of that bw step), BOLD written when `tr`.
         auto bw_pair = [&](int pr, float z0, float z1, bool tr, int bi) {
-            uint32_t w[16];  // x, F, N, Q, then their lo parts, of simulation 2 pr, then of 2 pr + 1
+            uint32_t w[16];
             const uint32_t col = t_lane + COL_BWT + (wg * SPT + 2 * pr) * 8;
             tmem_ld16(col, w);
-            float2 v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = make_float2(__uint_as_float(w[i]), __uint_as_float(w[8 + i]));
-            if (act) bw_step32x2(v, make_float2(z0, z1), bw);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                w[i] = __float_as_uint(v[i].x);
-                w[8 + i] = __float_as_uint(v[i].y);
-            }
+            double x[2], f[2], nu[2], q[2];
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
+                x[u] = __hiloint2double((int)w[8 * u + 1], (int)w[8 * u + 0]);
+                f[u] = __hiloint2double((int)w[8 * u + 3], (int)w[8 * u + 2]);
+                nu[u] = __hiloint2double((int)w[8 * u + 5], (int)w[8 * u + 4]);
+                q[u] = __hiloint2double((int)w[8 * u + 7], (int)w[8 * u + 6]);
+            }
+            if (act) bw_step64x2(x, f, nu, q, (double)z0, (double)z1, bw);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                w[8 * u + 0] = (uint32_t)__double2loint(x[u]); w[8 * u + 1] = (uint32_t)__double2hiint(x[u]);
+                w[8 * u + 2] = (uint32_t)__double2loint(f[u]); w[8 * u + 3] = (uint32_t)__double2hiint(f[u]);
+                w[8 * u + 4] = (uint32_t)__double2loint(nu[u]); w[8 * u + 5] = (uint32_t)__double2hiint(nu[u]);
+                w[8 * u + 6] = (uint32_t)__double2loint(q[u]); w[8 * u + 7] = (uint32_t)__double2hiint(q[u]);
                 const int sim = sims[2 * pr + u];
                 if (tr && act && sim >= 0 && bi < a.bold_len)  // no slot for a sample past bold_len
-                    a.bold[(size_t)sim * a.bold_len * n + (size_t)bi * n + j] =
-                        u ? bold32(v[2].y, v[6].y, v[3].y, v[7].y, bw) : bold32(v[2].x, v[6].x, v[3].x, v[7].x, bw);
+                    a.bold[(size_t)sim * a.bold_len * n + (size_t)bi * n + j] = bold64(q[u], nu[u], bw);
             }
             tmem_st16(col, w);
         };

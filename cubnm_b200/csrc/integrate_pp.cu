@@ -22,10 +22,9 @@
 //    commits them to a second mbarrier that the update threads wait on.
 //  * The node state (S_E, S_I of 16 simulations) lives in registers; the model
 //    parameters of all 64 simulations live in TMEM (5 columns per simulation),
-//    read per pair each step; the Balloon-Windkessel state, in the FP32
-//    deviation form of tc_common.cuh (x, f - 1, nu - 1, q - 1 as FP32 hi / lo
-//    pairs), lives in a per-CTA global scratch that stays in L2 (2 KB per node
-//    for the 64 simulations), updated once per bw step for one simulation pair per inner
+//    read per pair each step; the FP64 Balloon-Windkessel state (x, f, nu, q)
+//    lives in a per-CTA global scratch that stays in L2 (2 KB per node for the 64
+//    simulations), updated once per bw step for one simulation pair per inner
 //    step (after the halves' updates, while the next GEMMs run), staggered
 //    between warpgroups so that their loads spread over the bw step.  The time-averaged states are
 //    accumulated in shared memory (FP32) and written once per simulation.
@@ -148,12 +147,12 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
 
     // constants read from the parameter space where they are used (precomputed on the host)
     const typename M::K &K = *reinterpret_cast<const typename M::K *>(a.k32);
-    const BW32 &bw = a.bw32;
+    const BW64 &bw = a.bwf;
     const size_t rstride = (size_t)a.n_sims * n;
     const size_t ext = a.states_ts ? (size_t)n * a.states_len : (size_t)n;
     const int steps = a.bw_it * a.inner_it;
     // this CTA's Balloon-Windkessel scratch: [h][g][pr][x, f, nu, q][node] of simulation pairs
-    float4 *bws = reinterpret_cast<float4 *>(a.bw_scratch) + (size_t)blockIdx.x * (2 * 4 * 4 * 4) * n;
+    double2 *bws = reinterpret_cast<double2 *>(a.bw_scratch) + (size_t)blockIdx.x * (2 * 4 * 4 * 4) * n;
 
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const int *wd = work + (size_t)w * (1 + PP_SIMS);
@@ -218,9 +217,11 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
             if (act) {
 #pragma unroll
                 for (int p = 0; p < NPAIR; ++p) {
-                    float4 *b = bws + (size_t)(((WS ? h_own : (p >> 2))) * 16 + g * 4 + (p & 3)) * 4 * n + j;
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) b[c * n] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // x = f-1 = nu-1 = q-1 = 0
+                    double2 *b = bws + (size_t)(((WS ? h_own : (p >> 2))) * 16 + g * 4 + (p & 3)) * 4 * n + j;
+                    b[0] = make_double2(0.0, 0.0);
+                    b[n] = make_double2(1.0, 1.0);
+                    b[2 * n] = make_double2(1.0, 1.0);
+                    b[3 * n] = make_double2(1.0, 1.0);
                 }
             }
             if (a.ext_out && !a.states_ts && act) {  // state sums start at zero
@@ -325,37 +326,36 @@ __device__ __forceinline__ void pp_body(const IntegrateArgs &a, const int *work,
             float nz1 = (act && M::NN > 1) ? __ldg(nrow + 1) : 0.0f;
             bool aborted = false, pend = false, pend_tr = false;
             int pend_bi = 0;
-            float4 bwx[4];  // Balloon-Windkessel state of the pair being updated: {x, F}, {N, Q}, then their lo parts
+            double2 bwx[4];  // Balloon-Windkessel state of the pair being updated
             const int stagger = (2 * g + (WS ? 5 * h_own : 0)) % a.inner_it;
             auto half_of = [&](int p) { return WS ? h_own : (p >> 2); };
             auto bw_ptr = [&](int p) { return bws + (size_t)(half_of(p) * 16 + g * 4 + (p & 3)) * 4 * n + j; };
             auto bw_load = [&](int p) {
                 if (!act || !live[half_of(p)]) return;
-                const float4 *b = bw_ptr(p);
+                const double2 *b = bw_ptr(p);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) bwx[c] = __ldcg(b + (size_t)c * n);
             };
             // one bw step of pair p (inputs: z of the previous bw step), BOLD at TR
             auto bw_do = [&](int p) {
                 if (!act || !live[half_of(p)]) return;
-                float2 v[8];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    v[2 * c] = make_float2(bwx[c].x, bwx[c].y);
-                    v[2 * c + 1] = make_float2(bwx[c].z, bwx[c].w);
-                }
-                const float2 z = make_float2(zbuf[(2 * p) * NUPD + tid], zbuf[(2 * p + 1) * NUPD + tid]);
-                bw_step32x2(v, z, bw);
-                float4 *b = bw_ptr(p);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) __stcg(b + (size_t)c * n, make_float4(v[2 * c].x, v[2 * c].y, v[2 * c + 1].x, v[2 * c + 1].y));
+                double x[2] = {bwx[0].x, bwx[0].y}, f[2] = {bwx[1].x, bwx[1].y};
+                double nu[2] = {bwx[2].x, bwx[2].y}, q[2] = {bwx[3].x, bwx[3].y};
+                const float z0 = zbuf[(2 * p) * NUPD + tid], z1 = zbuf[(2 * p + 1) * NUPD + tid];
+                bw_step64_contracted(x[0], f[0], nu[0], q[0], (double)z0, bw);
+                bw_step64_contracted(x[1], f[1], nu[1], q[1], (double)z1, bw);
+                double2 *b = bw_ptr(p);
+                __stcg(b, make_double2(x[0], x[1]));
+                __stcg(b + n, make_double2(f[0], f[1]));
+                __stcg(b + 2 * n, make_double2(nu[0], nu[1]));
+                __stcg(b + 3 * n, make_double2(q[0], q[1]));
                 if (pend_tr && pend_bi < a.bold_len) {  // no slot for a sample past bold_len
 #pragma unroll
                     for (int u = 0; u < 2; ++u) {
                         const int sim = wd[1 + half_of(p) * PP_TN + g * PP_SPT + 2 * (p & 3) + u];
                         if (sim >= 0)
                             a.bold[(size_t)sim * a.bold_len * n + (size_t)pend_bi * n + j] =
-                                u ? bold32(v[2].y, v[6].y, v[3].y, v[7].y, bw) : bold32(v[2].x, v[6].x, v[3].x, v[7].x, bw);
+                                bold64(q[u], nu[u], bw);
                     }
                 }
             };
@@ -536,7 +536,7 @@ bool pp_supported(int model, int nodes, bool has_delay) {
     return model == MODEL_RWW;
 }
 
-size_t pp_bw_scratch_bytes(int nodes, int grid) { return sizeof(float4) * (size_t)grid * 2 * 4 * 4 * 4 * nodes; }
+size_t pp_bw_scratch_bytes(int nodes, int grid) { return sizeof(double2) * (size_t)grid * 2 * 4 * 4 * 4 * nodes; }
 
 cudaError_t launch_integrate_pp(int model, const IntegrateArgs &a, cudaStream_t st, int *launches) {
     if (launches) ++*launches;

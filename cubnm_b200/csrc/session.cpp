@@ -915,12 +915,13 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         has_delay = *std::max_element(h_max_delay.begin(), h_max_delay.end()) > 0;
     }
     // FP32 kernels: the tensor-core tiles take shared-SC batches without delays or
-    // numerical FIC at <= 128 nodes; everything else runs on the per-simulation
-    // kernel, which measured faster than the lane kernel on every delayed and
-    // large-network shape (1,000-node WC: 343 vs 218 sims x sim-s / s; 400-node
-    // rWW: 1,103 vs 435; 200-node rWW, 512 sims: 11,645 vs 1,593).  The lane kernel
-    // runs the G tangent, and when CBNM_FP32_KERNEL=lanes or the tuner picks it;
-    // CBNM_FP32_KERNEL=simt forces the per-simulation kernel everywhere.
+    // numerical FIC at <= 128 nodes.  Delayed networks of more than 512 nodes, with
+    // at least half as many 16-simulation groups as SMs, take the lane kernel
+    // (1,000-node WC, 2,048 sims: 440 vs 343 sims x sim-s / s); everything else runs
+    // on the per-simulation kernel, which measured faster there (400-node rWW with
+    // delays: 1,103 vs 435; 200-node rWW without, 512 sims: 11,645 vs 1,593).  The
+    // lane kernel also runs the G tangent, and when CBNM_FP32_KERNEL=lanes or the
+    // tuner picks it; CBNM_FP32_KERNEL=simt forces the per-simulation kernel.
     const char *fp32_kernel = std::getenv("CBNM_FP32_KERNEL");
     const bool force_simt = fp32_kernel && std::string(fp32_kernel) == "simt";
     const bool force_lanes = fp32_kernel && std::string(fp32_kernel) == "lanes";
@@ -960,7 +961,8 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
     }
     const bool use_tc = variant == V_DEFAULT ? (!tan_bold && !force_simt && tc_ok)
                                              : (variant == V_PP || variant == V_PPWS || variant == V_V5);
-    bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (tan_bold || (force_lanes && !use_tc)))
+    const bool lanes_default = has_delay && n > 512 && 2 * ((N + 15) / 16) >= sm_count() && !force_simt;
+    bool use_lanes = variant == V_DEFAULT ? (lanes_ok && (tan_bold || ((force_lanes || lanes_default) && !use_tc)))
                                           : (variant == V_LANES || variant == V_LANES512);
     const int lanes_threads = variant == V_LANES512 ? 512 : 1024;
     if (t_round && !t_round_resolved && !(use_lanes && lanes_threads == 1024 && !tan_bold && g_batch_launch)) {
@@ -1041,22 +1043,6 @@ static void run_impl(Session *sp, const cbnm_run_args *a, cbnm_outputs *o, bool 
         f.omr = ia.bw.oneminrho;
         f.V0k1 = ia.bw.V_0 * ia.bw.k1; f.V0k2 = ia.bw.V_0 * ia.bw.k2; f.V0k3 = ia.bw.V_0 * ia.bw.k3;
         std::copy(ia.bw_binom, ia.bw_binom + 13, f.binom);
-        BW32 &g = ia.bw32;
-        const double rho = ia.bw.rho;
-        g.dt = (float)ia.bw.dt; g.kappa = (float)ia.bw.kappa; g.y = (float)ia.bw.y; g.dt_itau = (float)ia.bw.dt_itau;
-        g.c_omr = (float)((1.0 - rho) / rho); g.m_ln_omr = (float)(-std::log1p(-rho));
-        g.ialpha = (float)ia.bw.ialpha; g.log2_omr = (float)std::log2(1.0 - rho); g.irho = (float)(1.0 / rho);
-        g.V0k1 = f.V0k1; g.V0k2 = f.V0k2; g.V0k3 = f.V0k3;
-        {
-            long double ca = 1.0L, cb = 1.0L;
-            const long double ea = (long double)ia.bw.ialpha, eb = ea - 1.0L;
-            for (int k = 1; k <= BW32_TERMS; ++k) {
-                ca = ca * (ea - (k - 1)) / k;
-                cb = cb * (eb - (k - 1)) / k;
-                g.a[k - 1] = (float)ca;
-                g.b[k - 1] = (float)cb;
-            }
-        }
         if (md.id == MODEL_RWW) {
             const RWW32::K k = RWW32::make(ia.K);
             static_assert(sizeof(k) <= sizeof(ia.k32), "FP32 constants");

@@ -397,144 +397,6 @@ __device__ __forceinline__ void bw_step64(double &x, double &f, double &nu, doub
     f = tmp_f;
 }
 
-// ---- Balloon-Windkessel step in FP32, deviation form.
-// f, nu and q stay near 1, so the state is kept as x and the deviations
-// F = f - 1, N = nu - 1, Q = q - 1, and each of the four as an FP32 pair
-// (hi, lo): a step adds an increment of ~1e-7 to a value of ~0.1, and in one
-// FP32 word the rounding of those additions would random-walk over a run (60,000
-// steps) to the size of a quiet network's BOLD fluctuations.  The pair keeps the
-// sum to ~1e-15; the nonlinear terms are evaluated on hi.  The step of bw_step64
-// rewritten in these variables (no approximation beyond the truncated series):
-//   x' = x + dt (z - kappa x - y F)
-//   F' = F + dt x'
-//   N' = N + dt/tau (F - P_a(N)),             P_a(N) = (1 + N)^(1/alpha) - 1
-//   Q' = Q + dt/tau ((A - 1) - (B - 1)), with
-//     A - 1 = f (1 - (1 - rho)^(1/f)) / rho - 1 = F - c (1 + F) expm1(u),
-//             c = (1 - rho) / rho, u = -ln(1 - rho) F / (1 + F)
-//     B - 1 = nu'^(1/alpha - 1) q - 1 = P_b + Q + P_b Q,  P_b = (1 + N')^(1/alpha - 1) - 1
-//   BOLD = V0 (-k1 Q + k2 (N - Q) / (1 + N) - k3 N), in FP64 from hi + lo.
-// For |N| <= 1/4 the powers are their binomial series to N^8 (1/alpha = 3.125 is
-// near an integer, so the coefficients fall fast: first omitted term < 1e-8
-// relative), and for |F| <= 1/2 expm1 is its Taylor series to u^8 (|u| <= 0.42,
-// first omitted term < 1e-7 of the result at the edge, far less inside); outside
-// those ranges the general forms through exp2f / log2f are used.  (rWW's BOLD
-// input S_E <= 1 keeps F below ~0.45 and N below ~0.15.)  Against the FP64 step
-// over 30,000 steps of inputs fluctuating by 1e-2 to 1e-4, the BOLD stays within
-// 2e-5 of its own standard deviation (one FP32 word per variable: 6e-3).
-__device__ __forceinline__ float bw32_series(float N, const float *c) {  // sum_{k=1..8} c_{k-1} N^k
-    float p = c[BW32_TERMS - 1];
-#pragma unroll
-    for (int k = BW32_TERMS - 2; k >= 0; --k) p = fmaf(p, N, c[k]);
-    return p * N;
-}
-__device__ __forceinline__ float bw32_pow1m(float N, const float *c, float e) {  // (1 + N)^e - 1
-    if (fabsf(N) <= 0.25f) return bw32_series(N, c);
-    return exp2f(e * log2f(1.0f + N)) - 1.0f;
-}
-__device__ __forceinline__ float bw32_expm1(float u) {  // sum_{k=1..8} u^k / k!
-    float p = 1.0f / 40320.0f;
-    p = fmaf(p, u, 1.0f / 5040.0f);
-    p = fmaf(p, u, 1.0f / 720.0f);
-    p = fmaf(p, u, 1.0f / 120.0f);
-    p = fmaf(p, u, 1.0f / 24.0f);
-    p = fmaf(p, u, 1.0f / 6.0f);
-    p = fmaf(p, u, 0.5f);
-    p = fmaf(p, u, 1.0f);
-    return p * u;
-}
-__device__ __forceinline__ float bw32_a1(float F, const BW32 &c) {  // A - 1
-    if (fabsf(F) <= 0.5f) {
-        const float u = c.m_ln_omr * F * __frcp_rn(1.0f + F);
-        return fmaf(-c.c_omr * bw32_expm1(u), 1.0f + F, F);
-    }
-    const float E = exp2f(c.log2_omr / (1.0f + F));
-    return (1.0f + F) * (1.0f - E) * c.irho - 1.0f;
-}
-// (hi, lo) += d, renormalised (two Fast2Sum steps) so that lo stays below half an
-// ulp of hi; every operation rounds once (no contraction).
-__device__ __forceinline__ void bw32_acc(float &hi, float &lo, float d) {
-    const float s = __fadd_rn(hi, d);
-    lo = __fadd_rn(lo, __fsub_rn(d, __fsub_rn(s, hi)));
-    hi = __fadd_rn(s, lo);
-    lo = __fsub_rn(lo, __fsub_rn(hi, s));
-}
-// v = {x, F, N, Q, x_lo, F_lo, N_lo, Q_lo}
-__device__ __forceinline__ void bw_step32(float (&v)[8], float z, const BW32 &c) {
-    const float dx = c.dt * fmaf(-c.y, v[1], fmaf(-c.kappa, v[0], z));
-    bw32_acc(v[0], v[4], dx);
-    const float dF = c.dt * v[0];
-    const float dN = c.dt_itau * (v[1] - bw32_pow1m(v[2], c.a, c.ialpha));
-    const float A1 = bw32_a1(v[1], c);
-    bw32_acc(v[2], v[6], dN);
-    const float P = bw32_pow1m(v[2], c.b, c.ialpha - 1.0f);
-    const float dQ = c.dt_itau * (A1 - fmaf(P, v[3], P + v[3]));
-    bw32_acc(v[3], v[7], dQ);
-    bw32_acc(v[1], v[5], dF);
-}
-
-// The same step for a simulation pair, two lanes per FFMA2 / FADD2; a pair
-// outside the series' range takes the scalar step.  v: the eight variables of
-// bw_step32, .x of the first simulation and .y of the second.
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }  // a - b, exact
-// sum_{k=1..8} c_{k-1} N^k by Estrin's scheme (dependency depth 4 instead of
-// Horner's 8: the step runs while the update warps wait on the GEMM, where its
-// latency, not its instruction count, is what costs)
-__device__ __forceinline__ float2 bw32_series2(float2 N, const float *c) {
-    const float2 N2 = __fmul2_rn(N, N), N4 = __fmul2_rn(N2, N2);
-    const float2 q0 = __ffma2_rn(f2(c[1]), N, f2(c[0])), q1 = __ffma2_rn(f2(c[3]), N, f2(c[2]));
-    const float2 q2 = __ffma2_rn(f2(c[5]), N, f2(c[4])), q3 = __ffma2_rn(f2(c[7]), N, f2(c[6]));
-    const float2 r0 = __ffma2_rn(q1, N2, q0), r1 = __ffma2_rn(q3, N2, q2);
-    return __fmul2_rn(__ffma2_rn(r1, N4, r0), N);
-}
-__device__ __forceinline__ float2 bw32_expm12(float2 u) {  // sum_{k=1..8} u^k / k!, Estrin
-    const float2 u2 = __fmul2_rn(u, u), u4 = __fmul2_rn(u2, u2);
-    const float2 q0 = __ffma2_rn(f2(0.5f), u, f2(1.0f)), q1 = __ffma2_rn(f2(1.0f / 24.0f), u, f2(1.0f / 6.0f));
-    const float2 q2 = __ffma2_rn(f2(1.0f / 720.0f), u, f2(1.0f / 120.0f));
-    const float2 q3 = __ffma2_rn(f2(1.0f / 40320.0f), u, f2(1.0f / 5040.0f));
-    const float2 r0 = __ffma2_rn(q1, u2, q0), r1 = __ffma2_rn(q3, u2, q2);
-    return __fmul2_rn(__ffma2_rn(r1, u4, r0), u);
-}
-__device__ __forceinline__ void bw32_acc2(float2 &hi, float2 &lo, float2 d) {
-    const float2 s = __fadd2_rn(hi, d);
-    lo = __fadd2_rn(lo, sub2(d, sub2(s, hi)));
-    hi = __fadd2_rn(s, lo);
-    lo = sub2(lo, sub2(hi, s));
-}
-// The terms that depend on an updated variable (F' on x', Q' on N') read the plain
-// FP32 sum of the old value and its increment, so the four compensated additions,
-// independent of each other, come last and off the dependency chain.
-__device__ __forceinline__ void bw_step32x2(float2 (&v)[8], float2 z, const BW32 &c) {
-    const bool in_range = fmaxf(fabsf(v[2].x), fabsf(v[2].y)) <= 0.2f && fmaxf(fabsf(v[1].x), fabsf(v[1].y)) <= 0.5f;
-    if (!in_range) {  // N' stays within 1/4 when |N| <= 0.2, so the pair path needs no second check
-        float a[8], b[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) { a[i] = v[i].x; b[i] = v[i].y; }
-        bw_step32(a, z.x, c);
-        bw_step32(b, z.y, c);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = make_float2(a[i], b[i]);
-        return;
-    }
-    const float2 dx = __fmul2_rn(f2(c.dt), __ffma2_rn(f2(-c.y), v[1], __ffma2_rn(f2(-c.kappa), v[0], z)));
-    const float2 dF = __fmul2_rn(f2(c.dt), __fadd2_rn(v[0], dx));
-    const float2 dN = __fmul2_rn(f2(c.dt_itau), sub2(v[1], bw32_series2(v[2], c.a)));
-    const float2 F1 = __fadd2_rn(v[1], f2(1.0f));
-    const float2 u = __fmul2_rn(__fmul2_rn(f2(c.m_ln_omr), v[1]), make_float2(__frcp_rn(F1.x), __frcp_rn(F1.y)));
-    const float2 A1 = __ffma2_rn(__fmul2_rn(f2(-c.c_omr), bw32_expm12(u)), F1, v[1]);
-    const float2 P = bw32_series2(__fadd2_rn(v[2], dN), c.b);
-    const float2 dQ = __fmul2_rn(f2(c.dt_itau), sub2(A1, __ffma2_rn(P, v[3], __fadd2_rn(P, v[3]))));
-    bw32_acc2(v[0], v[4], dx);
-    bw32_acc2(v[1], v[5], dF);
-    bw32_acc2(v[2], v[6], dN);
-    bw32_acc2(v[3], v[7], dQ);
-}
-
-// BOLD of the deviation state (hi, lo of N and Q), in FP64
-__device__ __forceinline__ double bold32(float N, float Nl, float Q, float Ql, const BW32 &c) {
-    const double n = (double)N + (double)Nl, q = (double)Q + (double)Ql;
-    return fma(-c.V0k1, q, fma(c.V0k2, (n - q) / (1.0 + n), -c.V0k3 * n));
-}
-
 // BOLD = V0 (k1 (1 - q) + k2 (1 - q / nu) + k3 (1 - nu))  (bnm.cpp:316-335)
 __device__ __forceinline__ double bold64(double q, double nu, const BW64 &c) {
     double b = __dmul_rn(c.V0k1, __dsub_rn(1.0, q));
