@@ -44,8 +44,10 @@ DURATION_S = 60
 # dram__bytes_read.sum + dram__bytes_write.sum of one integrator launch of the default
 # workload, from an ncu capture of one launch on a reduced case scaled by the
 # simulated node-steps (profiles/ names the capture); None until measured
-TRAFFIC_DEFAULT_WORKLOAD = None
-TRAFFIC_SOURCE = None
+TRAFFIC_DEFAULT_WORKLOAD = 6.242e9
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_integrate_tc launch on 9,472 sims x "
+                  "8 s (240.6 MB), scaled by node-steps to 32,768 x 60 s "
+                  "(profiles/k_integrate_tc_rww_9472x8s_counters.md)")
 # FP32 flops of one rWW node update (rww.cpp:194-232): I_E 8, I_I 4, the two affine
 # rate arguments 4, the two rates (without their exp) 6, dS_E 8, dS_I 6, the two
 # state additions 2
@@ -277,7 +279,8 @@ def run_ours(opts, rank, world, local_rank):
     issued = 3 * 2.0 * 128 * (((NODES + 15) // 16) * 16) * (n_sims * 1.0) * (opts.duration * 1e4)  # BF16x3 MMA work
     fp32_flops = RWW_FP32_FLOPS * node_steps
     traffic, traffic_src = opts.traffic, "--traffic" if opts.traffic is not None else None
-    if traffic is None and n_sims == N_SIMS and opts.duration == DURATION_S and opts.precision == "fp32":
+    if (traffic is None and n_sims == N_SIMS and opts.duration == DURATION_S and opts.precision == "fp32"
+            and core.last_integrator() == "tc1"):  # the capture is of the single-tile kernel
         traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, TRAFFIC_SOURCE
     roof = {"bound": "fp32", "achieved": fp32_flops / integ / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
             "frac": fp32_flops / integ / 1e12 / fp32_peak,
