@@ -145,10 +145,11 @@ def _delayed_args(model, N, nodes, duration_s, seed, precision, G):
 
 
 @pytest.mark.parametrize("model,G", [("WC", [0.4, 1.2, 1.8]), ("rWW", [0.5, 1.5, 3.0])])
-def test_tangent_dG_matches_fp64_finite_differences(model, G):
+def test_tangent_dG_matches_fp64_finite_differences(model, G, monkeypatch):
     """dL/dG of L = sum(w * BOLD) (fixed random weights) and of the fit loss, from
     dBOLD/dG of the tangent integrator (FP32 state, delays, 6 m/s), against central
-    differences of the FP64 path.  The tangent run's BOLD is the plain FP32 run's.
+    differences of the FP64 path.  The tangent run's BOLD is the plain FP32 lane
+    kernel run's.
 
     Every G here leaves the trajectory non-chaotic: on this network WC at G = 2.5
     is chaotic (a 1e-9 relative change of G moves the FP64 BOLD by 5e-3 within
@@ -159,7 +160,10 @@ def test_tangent_dG_matches_fp64_finite_differences(model, G):
     N, nodes, dur = 3, 24, 8
     G = np.array(G)
     bold, dG = grad.bold_and_dG(_delayed_args(model, N, nodes, dur, 11, "fp32", G))
+    # the tangent integrates on the lane kernel: its value path is that kernel's plain run
+    monkeypatch.setenv("CBNM_FP32_KERNEL", "lanes")
     plain = core.run_simulations(*_delayed_args(model, N, nodes, dur, 11, "fp32", G))["sim_bold"]
+    monkeypatch.delenv("CBNM_FP32_KERNEL")
     np.testing.assert_array_equal(bold.cpu().numpy().reshape(N, -1), plain)
     w = np.random.default_rng(2).standard_normal(bold.shape[1:])
     tan = (dG.cpu().numpy() * w).sum(axis=(1, 2))
