@@ -409,11 +409,11 @@ C2_DURATIONS = (60, 300, 600, 900)
 def c2_groups(scale, precision="fp32", sims_per_group=512):
     """Uneven batch: 8,192 rWW simulations over node counts x durations (16 groups of
     512), delays from 3-D points in a 70-mm sphere x 1.3 at 6 m/s, SC at 20 %, regional
-    w_p = w_p0 + w_p1 map.  Durations divided by `scale`."""
+    w_p = w_p0 + w_p1 map.  Durations divided by `scale` (at least 4 s)."""
     from cubnm_b200 import synthetic
     groups = []
     for gi, (nodes, dur) in enumerate([(n, d) for n in C2_NODES for d in C2_DURATIONS]):
-        d = max(2, int(round(dur / scale)))
+        d = max(4, int(round(dur / scale)))  # at least 4 s: with fewer volumes no FC window fits
         rng = np.random.default_rng(500 + gi)
         N = sims_per_group
         remove = min(10, d // 4)
@@ -430,6 +430,28 @@ def c2_groups(scale, precision="fp32", sims_per_group=512):
         a[11] = True
         groups.append(a)
     return groups
+
+
+def c0_args():
+    """The README grid: rWW 4 x 5 x 5 = 100 sims (G x w_p x J_N), 100 nodes, 60 s, FP64."""
+    from cubnm_b200 import synthetic
+    G, wp, jn = synthetic.rww_grid()
+    return list(synthetic.synthetic_args("rWW", N=100, nodes=100, duration_s=60, seed=0, G=G, w_p=wp, J_N=jn,
+                                         precision="fp64"))
+
+
+def c3_args(n_sims=512, duration_s=300):
+    """The gradient configuration: rWW, 200 nodes, SC at 25 %, FP32, FC + FCD w30 / s5;
+    G and J_N uniform over the reference's bounds.  Returns (SC [200, 200], args)."""
+    from cubnm_b200 import synthetic
+    nodes = 200
+    sc = synthetic.synthetic_sc(nodes, 0.25, 3)
+    rng = np.random.default_rng(33)
+    args = list(synthetic.synthetic_args("rWW", N=n_sims, nodes=nodes, duration_s=duration_s, seed=3, density=0.25,
+                                         G=rng.uniform(0.001, 10, n_sims), J_N=rng.uniform(0.001, 0.5, n_sims),
+                                         precision="fp32", window_size=30, window_step=5, bold_remove_s=30))
+    args[1] = np.ascontiguousarray(sc.ravel())[None, :]
+    return sc, args
 
 
 def c4_args(n_sims, duration_s, precision="fp32"):
@@ -524,9 +546,7 @@ def run_config(opts):
         return step, bufs
 
     if opts.config == "c0":
-        G, wp, jn = synthetic.rww_grid()
-        args = list(synthetic.synthetic_args("rWW", N=100, nodes=100, duration_s=60, seed=0, G=G, w_p=wp, J_N=jn,
-                                             precision="fp64"))
+        args = c0_args()
         workload = "README grid: rWW 4x5x5 = 100 sims, 100 nodes, 60 s, FP64, FC+FCD w10/s2, no FIC"
         sim_s = 100 * 60
         step, _ = device_runner(args)
@@ -597,12 +617,7 @@ def run_config(opts):
         extra["scale"] = scale
     elif opts.config == "c3":
         nodes, N, dur = 200, 512, 300
-        sc = synthetic.synthetic_sc(nodes, 0.25, 3)
-        rng = np.random.default_rng(33)
-        args = list(synthetic.synthetic_args("rWW", N=N, nodes=nodes, duration_s=dur, seed=3, density=0.25,
-                                             G=rng.uniform(0.001, 10, N), J_N=rng.uniform(0.001, 0.5, N),
-                                             precision="fp32", window_size=30, window_step=5, bold_remove_s=30))
-        args[1] = np.ascontiguousarray(sc.ravel())[None, :]
+        sc, args = c3_args(N, dur)
         workload = "gradient config: rWW 512 sims, 200 nodes, 300 s, SC 25%, FP32, FC+FCD w30/s5"
         sim_s = N * dur
         step, _ = device_runner(args)
@@ -636,7 +651,8 @@ def run_config(opts):
         emp = synthetic.synthetic_emp_bold(nodes, dur, 7)
         efc = torch.from_numpy(utils.calculate_fc(emp)).to(dev)
         efcd = torch.from_numpy(utils.calculate_fcd(emp, 30, 5)).to(dev)
-        G = torch.tensor(rng.uniform(0.5, 3, gs), dtype=torch.float64, device=dev, requires_grad=True)
+        G = torch.tensor(np.random.default_rng(34).uniform(0.5, 3, gs), dtype=torch.float64, device=dev,
+                         requires_grad=True)
         wp = torch.full((gs, nodes), 1.0, dtype=torch.float64, device=dev, requires_grad=True)
         jn = torch.full((gs, nodes), 0.15, dtype=torch.float64, device=dev, requires_grad=True)
         wie = torch.ones((gs, nodes), dtype=torch.float64, device=dev)
