@@ -522,6 +522,26 @@ def config_roofline(args, integrate_ms, delayed, fp32_peak=None):
                                      f"{node_steps:.3e} node-steps", "kernel": kernel, "kernel_ms": integrate_ms}
 
 
+def batch_roofline(groups, seconds):
+    """Roofline of an uneven batch (c2): the ring-buffer gather bytes of all groups
+    (4 bytes per nonzero of the target's SC column per node-step) over the batch's
+    wall time, against the measured HBM bandwidth.  The groups' integrators, FC and
+    copies run concurrently on their own streams, so there is no single launch to
+    time: this is a lower bound on the gathers' achieved bandwidth."""
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    b = 0.0
+    for g in groups:
+        N, n = g[14], g[15]
+        sc = np.asarray(g[1]).reshape(-1, n, n)
+        nnz = float(np.count_nonzero(sc[np.asarray(g[2], dtype=int)])) / (N * n)
+        b += N * n * (g[16] / g[20]) * nnz * 4.0
+    return {"bound": "hbm", "achieved": b / seconds / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": b / seconds / 1e9 / peaks["hbm_gbs"], "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "traffic": None, "algorithmic_bytes": b,
+            "work": "ring-buffer gathers of every group, 4 B per nonzero per node-step",
+            "basis": "whole-batch wall time (the groups' kernels run concurrently on their own streams)"}
+
+
 def run_config(opts):
     import torch
     from cubnm_b200 import _abi, core, synthetic, utils
@@ -613,7 +633,8 @@ def run_config(opts):
             per_group.append(g[14] * g[16] / 1000 / v)  # extrapolated seconds for the group
         cpu = {"value": sim_s / sum(per_group), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{2 * threads} sims x 2 s of each group, extrapolated per group to the batch"}
-        dtype, roof = "f32 (FP64 Balloon-Windkessel)", None
+        dtype = "f32 (FP64 Balloon-Windkessel)"
+        roof = batch_roofline(groups, ms / 1e3)
         extra["scale"] = scale
     elif opts.config == "c3":
         nodes, N, dur = 200, 512, 300

@@ -44,3 +44,16 @@ def test_c3_and_c4():
     for dur in (4, 10):
         s = _sizes(bench.c4_args(16, dur))
         assert s.bold_len == dur
+
+
+def test_batch_roofline_sums_the_groups():
+    groups = bench.c2_groups(15.0, sims_per_group=4)
+    r = bench.batch_roofline(groups, 2.0)
+    expect = 0.0
+    for g in groups:
+        n = g[15]
+        nnz = np.count_nonzero(np.asarray(g[1]).reshape(n, n)) / n
+        expect += g[14] * n * (g[16] / g[20]) * nnz * 4.0
+    assert abs(r["algorithmic_bytes"] - expect) <= 1e-9 * expect
+    assert abs(r["achieved"] - expect / 2.0 / 1e9) <= 1e-9 * r["achieved"]
+    assert r["bound"] == "hbm" and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
