@@ -280,7 +280,7 @@ def run_ours(opts, rank, world, local_rank):
     fp32_flops = RWW_FP32_FLOPS * node_steps
     traffic, traffic_src = opts.traffic, "--traffic" if opts.traffic is not None else None
     if (traffic is None and n_sims == N_SIMS and opts.duration == DURATION_S and opts.precision == "fp32"
-            and core.last_integrator() == "tc1"):  # the capture is of the single-tile kernel
+            and integrator == "tc1"):  # the capture is of the single-tile kernel
         traffic, traffic_src = TRAFFIC_DEFAULT_WORKLOAD, TRAFFIC_SOURCE
     roof = {"bound": "fp32", "achieved": fp32_flops / integ / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
             "frac": fp32_flops / integ / 1e12 / fp32_peak,
@@ -294,7 +294,7 @@ def run_ours(opts, rank, world, local_rank):
                        "mma_issued_tflops": issued / integ / 1e12},
             "traffic": traffic, "traffic_source": traffic_src,
             "algorithmic_bytes": N_SIMS * NODES * DURATION_S * 8.0 if n_sims == N_SIMS else None,
-            "kernel": KERNEL_OF.get(core.last_integrator(), core.last_integrator()), "kernel_ms": integ * 1e3,
+            "kernel": KERNEL_OF.get(integrator, integrator), "kernel_ms": integ * 1e3,
             "note": "per-pipe utilisation of this kernel: profiles/ (ncu)"}
 
     line = {
